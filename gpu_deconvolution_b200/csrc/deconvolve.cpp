@@ -1,0 +1,338 @@
+// Plan objects and the plane-streaming driver behind the public deconvolution
+// API (fmvd_initialize / deconvolve_planes / destroy, files entry point).
+//
+// The reference streams one plane per CUDA stream slot through a ring of
+// nstreams slots, 8 launches per view and iteration
+// (fmvd_deconvolve.impl.cpp:205-300).  Here planes are gathered into batches
+// of 2 * pairs_cap planes (pinned host buffers, two batch slots), copied with
+// one transfer per view and direction, and deconvolved together by the engine.
+// While batch k computes on the device, the host pulls batch k+1 from the
+// datasource and hands batch k-1 to the datasink, so host I/O overlaps the
+// device work; uploads and downloads run on their own streams.
+#include "fmvd_internal.h"
+
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+
+namespace fmvd {
+
+namespace {
+
+template <typename S>
+struct Traits;
+template <>
+struct Traits<unsigned short> {
+    using plan_t = fmvd_plan_cuda_16;
+    using source_t = datasource_16_t;
+    using sink_t = datasink_16_t;
+    static constexpr int bits = 16;
+};
+template <>
+struct Traits<unsigned char> {
+    using plan_t = fmvd_plan_cuda_8;
+    using source_t = datasource_8_t;
+    using sink_t = datasink_8_t;
+    static constexpr int bits = 8;
+};
+
+template <typename S>
+struct Streamer {
+    Engine *eng = nullptr;
+    int cap_planes = 0;
+    size_t plane = 0;
+    struct Slot {
+        S *h_in = nullptr, *d_in = nullptr, *h_out = nullptr, *d_out = nullptr;
+        std::vector<S *> view_ptrs;
+        int n = 0;
+        cudaEvent_t up = nullptr, done = nullptr, down = nullptr;
+    } slot[2];
+    cudaStream_t s_up = nullptr, s_comp = nullptr, s_down = nullptr;
+
+    bool init(Engine *e)
+    {
+        eng = e;
+        cap_planes = 2 * e->pairs_cap;
+        plane = (size_t)e->dims.dataH * e->dims.dataW;
+        const int V = e->dims.V;
+        bool ok = FMVD_CHECK(cudaStreamCreateWithFlags(&s_up, cudaStreamNonBlocking)) &&
+                  FMVD_CHECK(cudaStreamCreateWithFlags(&s_comp, cudaStreamNonBlocking)) &&
+                  FMVD_CHECK(cudaStreamCreateWithFlags(&s_down, cudaStreamNonBlocking));
+        for (int k = 0; k < 2 && ok; k++) {
+            Slot &sl = slot[k];
+            const size_t in_bytes = sizeof(S) * plane * cap_planes * V;
+            const size_t out_bytes = sizeof(S) * plane * cap_planes;
+            ok = FMVD_CHECK(cudaMallocHost(&sl.h_in, in_bytes)) && FMVD_CHECK(cudaMalloc(&sl.d_in, in_bytes)) &&
+                 FMVD_CHECK(cudaMallocHost(&sl.h_out, out_bytes)) && FMVD_CHECK(cudaMalloc(&sl.d_out, out_bytes)) &&
+                 FMVD_CHECK(cudaEventCreateWithFlags(&sl.up, cudaEventDisableTiming)) &&
+                 FMVD_CHECK(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming)) &&
+                 FMVD_CHECK(cudaEventCreateWithFlags(&sl.down, cudaEventDisableTiming));
+            if (ok) {
+                memset(sl.h_in, 0, in_bytes);
+                sl.view_ptrs.resize(V);
+                for (int v = 0; v < V; v++)
+                    sl.view_ptrs[v] = sl.h_in + (size_t)v * cap_planes * plane;
+            }
+        }
+        return ok;
+    }
+
+    void release()
+    {
+        for (auto &sl : slot) {
+            cudaFreeHost(sl.h_in);
+            cudaFree(sl.d_in);
+            cudaFreeHost(sl.h_out);
+            cudaFree(sl.d_out);
+            if (sl.up) cudaEventDestroy(sl.up);
+            if (sl.done) cudaEventDestroy(sl.done);
+            if (sl.down) cudaEventDestroy(sl.down);
+        }
+        if (s_up) cudaStreamDestroy(s_up);
+        if (s_comp) cudaStreamDestroy(s_comp);
+        if (s_down) cudaStreamDestroy(s_down);
+    }
+};
+
+template <typename S>
+struct Plan {
+    typename Traits<S>::plan_t pub;  // first member: the public struct
+    Streamer<S> st;
+};
+
+template <typename S>
+typename Traits<S>::plan_t *initialize(int dataH, int dataW, const float *const *h_Weights, float **h_Kernel,
+                                       int kernelH, int kernelW, int type, int nViews, int nstreams,
+                                       typename Traits<S>::source_t src, typename Traits<S>::sink_t sink,
+                                       int pairs_cap)
+{
+    if (nstreams < 1) {
+        report_error("fmvd: nstreams must be at least 1");
+        return nullptr;
+    }
+    Engine *e = engine_create(Traits<S>::bits, dataH, dataW, h_Weights, h_Kernel, kernelH, kernelW, type, nViews,
+                              pairs_cap);
+    if (!e)
+        return nullptr;
+    Plan<S> *p = new Plan<S>();
+    if (!p->st.init(e)) {
+        p->st.release();
+        engine_destroy(e);
+        delete p;
+        return nullptr;
+    }
+    auto &q = p->pub;
+    q.dataH = dataH;
+    q.dataW = dataW;
+    q.fftH = e->dims.H;
+    q.fftW = e->dims.W;
+    q.kernelH = kernelH;
+    q.kernelW = kernelW;
+    q.nViews = nViews;
+    q.nStreams = nstreams;
+    q.get_next_plane = src;
+    q.return_next_plane = sink;
+    q.engine = p;
+    return &p->pub;
+}
+
+template <typename S>
+void destroy(typename Traits<S>::plan_t *plan)
+{
+    if (!plan)
+        return;
+    Plan<S> *p = reinterpret_cast<Plan<S> *>(plan->engine);
+    cudaDeviceSynchronize();
+    Engine *e = p->st.eng;
+    p->st.release();
+    engine_destroy(e);
+    delete p;
+}
+
+template <typename S>
+void deconvolve_planes(const typename Traits<S>::plan_t *plan, int iterations)
+{
+    if (!plan)
+        return;
+    Plan<S> *p = reinterpret_cast<Plan<S> *>(plan->engine);
+    Streamer<S> &st = p->st;
+    Engine *e = st.eng;
+    const int V = e->dims.V;
+    const size_t plane = st.plane;
+    const int cap = st.cap_planes;
+    const size_t view_stride = plane * cap;
+    auto get = plan->get_next_plane;
+    auto put = plan->return_next_plane;
+
+    bool exhausted = false;
+    int obtained = 0;  // planes handed out by the source, plus unfilled quirk slots
+    // Fill a slot from the datasource.  The reference primes nstreams slots
+    // without looking at the return value (fmvd_deconvolve.impl.cpp:216-219),
+    // so a source holding fewer planes than nstreams still produces nstreams
+    // planes; the extra calls are made here once the source runs dry.
+    auto fill = [&](typename Streamer<S>::Slot &sl) {
+        sl.n = 0;
+        while (sl.n < cap) {
+            if (!exhausted) {
+                if (get(sl.view_ptrs.data(), (int)(sl.n * plane))) {
+                    sl.n++;
+                    obtained++;
+                    continue;
+                }
+                exhausted = true;
+            }
+            if (obtained >= plan->nStreams)
+                break;
+            for (int v = 0; v < V; v++)
+                memset(sl.view_ptrs[v] + sl.n * plane, 0, plane * sizeof(S));
+            get(sl.view_ptrs.data(), (int)(sl.n * plane));
+            sl.n++;
+            obtained++;
+        }
+    };
+
+    int cur = 0, prev = -1;
+    fill(st.slot[cur]);
+    while (true) {
+        auto &sl = st.slot[cur];
+        if (sl.n > 0) {
+            // upload: one copy per view, after the compute that last read this slot
+            if (!FMVD_CHECK(cudaStreamWaitEvent(st.s_up, sl.done, 0)))
+                return;
+            for (int v = 0; v < V; v++)
+                if (!FMVD_CHECK(cudaMemcpyAsync(sl.d_in + view_stride * v, sl.view_ptrs[v], sizeof(S) * plane * sl.n,
+                                                cudaMemcpyHostToDevice, st.s_up)))
+                    return;
+            FMVD_CHECK(cudaEventRecord(sl.up, st.s_up));
+            FMVD_CHECK(cudaStreamWaitEvent(st.s_comp, sl.up, 0));
+            engine_batch(e, sl.d_in, view_stride, sl.d_out, sl.n, iterations, st.s_comp);
+            if (!FMVD_CHECK(cudaGetLastError()))
+                return;
+            FMVD_CHECK(cudaEventRecord(sl.done, st.s_comp));
+            FMVD_CHECK(cudaStreamWaitEvent(st.s_down, sl.done, 0));
+            FMVD_CHECK(cudaMemcpyAsync(sl.h_out, sl.d_out, sizeof(S) * plane * sl.n, cudaMemcpyDeviceToHost,
+                                       st.s_down));
+            FMVD_CHECK(cudaEventRecord(sl.down, st.s_down));
+        }
+        // host work overlapping the device: next batch in, previous batch out
+        const int nxt = cur ^ 1;
+        auto &sn = st.slot[nxt];
+        if (prev >= 0) {
+            // slot nxt holds the previous batch: sink it before refilling
+            if (!FMVD_CHECK(cudaEventSynchronize(sn.down)))
+                return;
+            for (int i = 0; i < sn.n; i++)
+                put(sn.h_out + (size_t)i * plane);
+            sn.n = 0;
+        }
+        if (sl.n == 0)
+            break;
+        if (!FMVD_CHECK(cudaEventSynchronize(sn.up)))
+            return;
+        fill(sn);
+        prev = cur;
+        cur = nxt;
+        if (sn.n == 0) {
+            // nothing more: drain the batch just launched
+            if (!FMVD_CHECK(cudaEventSynchronize(sl.down)))
+                return;
+            for (int i = 0; i < sl.n; i++)
+                put(sl.h_out + (size_t)i * plane);
+            sl.n = 0;
+            break;
+        }
+    }
+}
+
+// fmvd_deconvolve_hdd.impl.cpp:16-76: the file source reads one plane per
+// view, the file sink writes one plane; nstreams is 3.
+template <typename S>
+struct FileIO {
+    static FILE **files;
+    static FILE *result;
+    static size_t planesize;
+    static int plane, nplanes, nviews;
+    static int source(S **data, int offset)
+    {
+        if (plane >= nplanes)
+            return 0;
+        for (int v = 0; v < nviews; v++)
+            if (fread(data[v] + offset, sizeof(S), planesize, files[v]) != planesize)
+                report_error("fmvd: short read from a data file");
+        plane++;
+        return 1;
+    }
+    static void sink(S *data) { fwrite(data, sizeof(S), planesize, result); }
+};
+template <typename S> FILE **FileIO<S>::files = nullptr;
+template <typename S> FILE *FileIO<S>::result = nullptr;
+template <typename S> size_t FileIO<S>::planesize = 0;
+template <typename S> int FileIO<S>::plane = 0;
+template <typename S> int FileIO<S>::nplanes = 0;
+template <typename S> int FileIO<S>::nviews = 0;
+
+template <typename S>
+void deconvolve_files(FILE **dataFiles, FILE *resultFile, int dataW, int dataH, int dataD, float **h_Weights,
+                      float **h_Kernel, int kernelH, int kernelW, int type, int nViews, int iterations)
+{
+    using IO = FileIO<S>;
+    IO::files = dataFiles;
+    IO::result = resultFile;
+    IO::planesize = (size_t)dataW * dataH;
+    IO::plane = 0;
+    IO::nplanes = dataD;
+    IO::nviews = nViews;
+    auto *plan = initialize<S>(dataH, dataW, h_Weights, h_Kernel, kernelH, kernelW, type, nViews, 3, IO::source,
+                               IO::sink, 0);
+    if (!plan)
+        return;
+    deconvolve_planes<S>(plan, iterations);
+    destroy<S>(plan);
+}
+
+} // namespace
+
+// ---------------------------------------------------------------- exports
+void *pinned_malloc(size_t size)
+{
+    void *p = nullptr;
+    if (!FMVD_CHECK(cudaMallocHost(&p, size)))
+        return nullptr;
+    return p;
+}
+
+void pinned_free(void *p) { cudaFreeHost(p); }
+
+fmvd_plan_cuda_16 *initialize_16(int dataH, int dataW, const float *const *w, float **k, int kH, int kW, int type,
+                                 int V, int nstreams, datasource_16_t src, datasink_16_t sink, int pairs_cap)
+{
+    return initialize<unsigned short>(dataH, dataW, w, k, kH, kW, type, V, nstreams, src, sink, pairs_cap);
+}
+
+fmvd_plan_cuda_8 *initialize_8(int dataH, int dataW, const float *const *w, float **k, int kH, int kW, int type,
+                               int V, int nstreams, datasource_8_t src, datasink_8_t sink, int pairs_cap)
+{
+    return initialize<unsigned char>(dataH, dataW, w, k, kH, kW, type, V, nstreams, src, sink, pairs_cap);
+}
+
+void deconvolve_planes_16(const fmvd_plan_cuda_16 *p, int it) { deconvolve_planes<unsigned short>(p, it); }
+void deconvolve_planes_8(const fmvd_plan_cuda_8 *p, int it) { deconvolve_planes<unsigned char>(p, it); }
+void destroy_16(fmvd_plan_cuda_16 *p) { destroy<unsigned short>(p); }
+void destroy_8(fmvd_plan_cuda_8 *p) { destroy<unsigned char>(p); }
+
+void deconvolve_files_16(FILE **f, FILE *r, int dW, int dH, int dD, float **w, float **k, int kH, int kW, int type,
+                         int V, int it)
+{
+    deconvolve_files<unsigned short>(f, r, dW, dH, dD, w, k, kH, kW, type, V, it);
+}
+
+void deconvolve_files_8(FILE **f, FILE *r, int dW, int dH, int dD, float **w, float **k, int kH, int kW, int type,
+                        int V, int it)
+{
+    deconvolve_files<unsigned char>(f, r, dW, dH, dD, w, k, kH, kW, type, V, it);
+}
+
+Engine *plan_engine_16(const fmvd_plan_cuda_16 *p) { return p ? reinterpret_cast<Plan<unsigned short> *>(p->engine)->st.eng : nullptr; }
+Engine *plan_engine_8(const fmvd_plan_cuda_8 *p) { return p ? reinterpret_cast<Plan<unsigned char> *>(p->engine)->st.eng : nullptr; }
+
+} // namespace fmvd

@@ -1,0 +1,452 @@
+// Affine trilinear resampler and transformed weight mask on sm_100a.
+//
+// Replaces transform_cuda_8/16 of the reference (fmvd_transform.impl.cu:77-224),
+// which binds the source to a 3-D texture and fetches every target voxel with
+// hardware trilinear filtering.  Here the source lives in plain device memory
+// (rows padded to 16 bytes) described by a 3-D TMA tensor map.  Each CTA
+// resamples a 32 x 8 tile of one target plane: since the map is affine, every
+// tile's source footprint has the same shape, so the host sizes one box that
+// covers it (with slack for rounding), one thread issues a single
+// cp.async.bulk.tensor load of that brick into shared memory (out-of-volume
+// texels arrive as zeros, the texture's border colour), and the threads
+// interpolate from shared memory.  The interpolation follows the texture
+// unit's linear filter: texel centres at i + 0.5, weights held with 8
+// fractional bits, values normalised by 2^bits - 1; output quantised as the
+// reference does, (sample)(v * 2^bits + 0.5) through a 32-bit integer.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+#include <vector>
+
+#include "fmvd_internal.h"
+#include "transform_kernels.h"
+
+namespace fmvd {
+
+namespace {
+
+constexpr int TX = 32, TY = 8;  // target tile
+
+struct Mat {
+    float m[12];
+};
+
+// rx = m0 x + m1 y + m2 z + m3 (fmvd_transform.impl.cu:41-43), same evaluation order
+__device__ __forceinline__ void apply(const Mat &M, int x, int y, int z, float &rx, float &ry, float &rz)
+{
+    rx = M.m[0] * x + M.m[1] * y + M.m[2] * z + M.m[3];
+    ry = M.m[4] * x + M.m[5] * y + M.m[6] * z + M.m[7];
+    rz = M.m[8] * x + M.m[9] * y + M.m[10] * z + M.m[11];
+}
+
+// Texel index and 1/256-quantised weight along one axis for source position r
+// (the reference fetches at r + 0.5 in unnormalised texture coordinates; the
+// filter works at xB = coordinate - 0.5).  The fractional part is rounded to
+// the nearest 1/256, halves up.
+__device__ __forceinline__ void tex_axis(float r, int &i, float &a)
+{
+    const float u = (float)((double)r + 0.5);
+    const float fx = (u - 0.5f) * 256.0f;
+    const float q = floorf(fx + 0.5f);
+    const float fi = floorf(q * (1.0f / 256.0f));
+    i = (int)fi;
+    a = (q - fi * 256.0f) * (1.0f / 256.0f);
+}
+
+template <typename S>
+__device__ __forceinline__ float to_sample_float(S v, float inv)
+{
+    return (float)v * inv;
+}
+
+template <typename S, int BITS>
+__device__ __forceinline__ S quantise(float v)
+{
+    // (SAMPLE)(v * 2^BITS + 0.5) as the reference compiles it: float product,
+    // double sum, conversion through a 32-bit unsigned integer, so a fetch of
+    // exactly 1.0 wraps to 0 (measured on the B200)
+    const double q = (double)(v * (float)(1 << BITS)) + 0.5;
+    return (S)__double2uint_rz(q);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+template <typename S, int BITS>
+__global__ void __launch_bounds__(TX *TY) resample_tma(const __grid_constant__ CUtensorMap tmap,
+                                                       const S *__restrict__ src, int w, int h, int d, size_t pitch,
+                                                       int tw, int th, int z0, const Mat M, int bx, int by, int bz,
+                                                       S *__restrict__ out, float *__restrict__ outf,
+                                                       int *__restrict__ status)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar;
+    S *brick = reinterpret_cast<S *>(smem_raw);
+    constexpr int XALIGN = 16 / sizeof(S);
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z = z0 + blockIdx.z;
+    const int tid = threadIdx.x;
+
+    // brick origin: minimum over the tile corners, one texel of slack
+    float mn[3] = {3.4e38f, 3.4e38f, 3.4e38f};
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        float r[3];
+        apply(M, x0 + (c & 1) * (TX - 1), y0 + (c >> 1) * (TY - 1), z, r[0], r[1], r[2]);
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            mn[k] = fminf(mn[k], r[k]);
+    }
+    int ox = (int)floorf(mn[0]) - 1;
+    ox = (ox >= 0) ? (ox / XALIGN) * XALIGN : -(((-ox) + XALIGN - 1) / XALIGN) * XALIGN;
+    const int oy = (int)floorf(mn[1]) - 1;
+    const int oz = (int)floorf(mn[2]) - 1;
+
+    const uint32_t bar_a = smem_u32(&bar);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const uint32_t bytes = (uint32_t)(bx * by * bz * sizeof(S));
+    if (tid == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes) : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+                smem_u32(brick)),
+            "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(ox), "r"(oy), "r"(oz), "r"(bar_a)
+            : "memory");
+    }
+    // bounded wait for the brick (phase 0)
+    uint32_t done = 0;
+    for (int spin = 0; spin < (1 << 22) && !done; spin++) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar_a)
+            : "memory");
+        if (!done && spin > 64)
+            __nanosleep(64);
+    }
+    const bool have_brick = done != 0;
+    if (!have_brick && tid == 0)
+        atomicExch(status, 1);
+
+    const int x = x0 + (tid % TX), y = y0 + (tid / TX);
+    if (x < tw && y < th) {
+        float rx, ry, rz;
+        apply(M, x, y, z, rx, ry, rz);
+        int ix, iy, iz;
+        float ax, ay, az;
+        tex_axis(rx, ix, ax);
+        tex_axis(ry, iy, ay);
+        tex_axis(rz, iz, az);
+        const float inv = 1.0f / (float)((1 << BITS) - 1);
+        const int lx = ix - ox, ly = iy - oy, lz = iz - oz;
+        float t[8];
+        if (have_brick && lx >= 0 && lx + 1 < bx && ly >= 0 && ly + 1 < by && lz >= 0 && lz + 1 < bz) {
+#pragma unroll
+            for (int c = 0; c < 8; c++)
+                t[c] = to_sample_float(brick[((lz + (c >> 2)) * by + (ly + ((c >> 1) & 1))) * bx + lx + (c & 1)], inv);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                const int sx = ix + (c & 1), sy = iy + ((c >> 1) & 1), sz = iz + (c >> 2);
+                const bool in = sx >= 0 && sx < w && sy >= 0 && sy < h && sz >= 0 && sz < d;
+                t[c] = in ? to_sample_float(__ldg(src + ((size_t)sz * h + sy) * pitch + sx), inv) : 0.f;
+            }
+        }
+        const float bx0 = 1.f - ax, by0 = 1.f - ay, bz0 = 1.f - az;
+        const float v = bz0 * (by0 * (bx0 * t[0] + ax * t[1]) + ay * (bx0 * t[2] + ax * t[3])) +
+                        az * (by0 * (bx0 * t[4] + ax * t[5]) + ay * (bx0 * t[6] + ax * t[7]));
+        const size_t oi = ((size_t)blockIdx.z * th + y) * tw + x;
+        if (out)
+            out[oi] = quantise<S, BITS>(v);
+        if (outf)
+            outf[oi] = v * (float)((1 << BITS) - 1);
+    }
+}
+
+// fmvd_transform.cu:19-67
+__global__ void mask_kernel(float *__restrict__ out, int z, int w, int h, int d, float zspacing, int tw, int th,
+                            float border, const Mat M)
+{
+    const int x = threadIdx.x + blockIdx.x * blockDim.x;
+    const int y = threadIdx.y + blockIdx.y * blockDim.y;
+    if (x >= tw || y >= th)
+        return;
+    float rx, ry, rz;
+    apply(M, x, y, z, rx, ry, rz);
+    float v = 0.f;
+    if (!(rx < 0 || rx >= w || ry < 0 || ry >= h || rz < 0 || rz >= d)) {
+        const float pi = 3.14159265358979323846f;
+        float dx = rx < w / 2 ? rx : w - rx;
+        float dy = ry < h / 2 ? ry : h - ry;
+        float dz = rz < d / 2 ? rz : d - rz;
+        dz *= zspacing;
+        v = 1.f;
+        if (dx < border)
+            v *= 0.5f * (1 - cosf(dx / border * pi));
+        if (dy < border)
+            v *= 0.5f * (1 - cosf(dy / border * pi));
+        if (dz < border)
+            v *= 0.5f * (1 - cosf(dz / border * pi));
+    }
+    out[(size_t)y * tw + x] = v;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+int ceil_i(float v) { return (int)ceilf(v); }
+
+} // namespace
+
+// Source volume in device memory: d planes of h rows, row pitch 'pitch'
+// samples (a multiple of 16 bytes).
+bool resample_device(int bits, const void *d_src, size_t pitch, int w, int h, int d, int tw, int th, int z0, int nz,
+                     const float *h_inverse, void *d_out, float *d_outf, int *d_status, cudaStream_t s)
+{
+    const size_t es = bits == 16 ? 2 : 1;
+    Mat M;
+    memcpy(M.m, h_inverse, sizeof(M.m));
+    const int xalign = (int)(16 / es);
+    // box covering one tile's footprint: extent + 2 texels for the filter and
+    // slack, plus the alignment of the x origin
+    int box[3];
+    for (int a = 0; a < 3; a++) {
+        const float ext = fabsf(M.m[4 * a]) * (TX - 1) + fabsf(M.m[4 * a + 1]) * (TY - 1);
+        box[a] = ceil_i(ext) + 4;
+    }
+    box[0] = ((box[0] + xalign - 1 + xalign - 1) / xalign) * xalign;
+    const size_t smem = (size_t)box[0] * box[1] * box[2] * es;
+    const bool boxes_ok = box[0] <= 256 && box[1] <= 256 && box[2] <= 256 && smem <= 96 * 1024;
+
+    CUtensorMap tmap;
+    memset(&tmap, 0, sizeof(tmap));
+    bool use_tma = boxes_ok && encode_fn() != nullptr;
+    if (use_tma) {
+        cuuint64_t gdim[3] = {(cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)d};
+        cuuint64_t gstride[2] = {(cuuint64_t)(pitch * es), (cuuint64_t)(pitch * es * h)};
+        cuuint32_t bdim[3] = {(cuuint32_t)box[0], (cuuint32_t)box[1], (cuuint32_t)box[2]};
+        cuuint32_t estride[3] = {1, 1, 1};
+        CUresult r = encode_fn()(&tmap, bits == 16 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8, 3,
+                                 const_cast<void *>(d_src), gdim, gstride, bdim, estride,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        use_tma = (r == CUDA_SUCCESS);
+    }
+    if (!use_tma) {
+        // no brick fits (extreme scaling): every voxel takes the direct path
+        box[0] = box[1] = box[2] = 0;
+    }
+    dim3 grid((tw + TX - 1) / TX, (th + TY - 1) / TY, nz);
+    const size_t shm = use_tma ? smem : 0;
+    if (bits == 16) {
+        auto k = resample_tma<unsigned short, 16>;
+        if (shm > 48 * 1024)
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+        if (use_tma) {
+            k<<<grid, TX * TY, shm, s>>>(tmap, (const unsigned short *)d_src, w, h, d, pitch, tw, th, z0, M, box[0],
+                                         box[1], box[2], (unsigned short *)d_out, d_outf, d_status);
+            rl_count_launch(1);
+        } else {
+            resample_direct(bits, d_src, pitch, w, h, d, tw, th, z0, nz, h_inverse, d_out, d_outf, s);
+        }
+    } else {
+        auto k = resample_tma<unsigned char, 8>;
+        if (shm > 48 * 1024)
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+        if (use_tma) {
+            k<<<grid, TX * TY, shm, s>>>(tmap, (const unsigned char *)d_src, w, h, d, pitch, tw, th, z0, M, box[0],
+                                         box[1], box[2], (unsigned char *)d_out, d_outf, d_status);
+            rl_count_launch(1);
+        } else {
+            resample_direct(bits, d_src, pitch, w, h, d, tw, th, z0, nz, h_inverse, d_out, d_outf, s);
+        }
+    }
+    return FMVD_CHECK(cudaGetLastError());
+}
+
+bool mask_device(float *d_out, int z, int w, int h, int d, float zspacing, int tw, int th, float border,
+                 const float *h_inverse, cudaStream_t s)
+{
+    Mat M;
+    memcpy(M.m, h_inverse, sizeof(M.m));
+    dim3 threads(32, 8);
+    dim3 grid((tw + 31) / 32, (th + 7) / 8);
+    mask_kernel<<<grid, threads, 0, s>>>(d_out, z, w, h, d, zspacing, tw, th, border, M);
+    rl_count_launch(1);
+    return FMVD_CHECK(cudaGetLastError());
+}
+
+// Direct-gather variant (no TMA brick): every texel read from global memory.
+template <typename S, int BITS>
+__global__ void resample_direct_kernel(const S *__restrict__ src, int w, int h, int d, size_t pitch, int tw, int th,
+                                       int z0, const Mat M, S *__restrict__ out, float *__restrict__ outf)
+{
+    const int x = blockIdx.x * TX + (threadIdx.x % TX), y = blockIdx.y * TY + (threadIdx.x / TX);
+    const int z = z0 + blockIdx.z;
+    if (x >= tw || y >= th)
+        return;
+    float rx, ry, rz;
+    apply(M, x, y, z, rx, ry, rz);
+    int ix, iy, iz;
+    float ax, ay, az;
+    tex_axis(rx, ix, ax);
+    tex_axis(ry, iy, ay);
+    tex_axis(rz, iz, az);
+    const float inv = 1.0f / (float)((1 << BITS) - 1);
+    float t[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        const int sx = ix + (c & 1), sy = iy + ((c >> 1) & 1), sz = iz + (c >> 2);
+        const bool in = sx >= 0 && sx < w && sy >= 0 && sy < h && sz >= 0 && sz < d;
+        t[c] = in ? to_sample_float(__ldg(src + ((size_t)sz * h + sy) * pitch + sx), inv) : 0.f;
+    }
+    const float bx0 = 1.f - ax, by0 = 1.f - ay, bz0 = 1.f - az;
+    const float v = bz0 * (by0 * (bx0 * t[0] + ax * t[1]) + ay * (bx0 * t[2] + ax * t[3])) +
+                    az * (by0 * (bx0 * t[4] + ax * t[5]) + ay * (bx0 * t[6] + ax * t[7]));
+    const size_t oi = ((size_t)blockIdx.z * th + y) * tw + x;
+    if (out)
+        out[oi] = quantise<S, BITS>(v);
+    if (outf)
+        outf[oi] = v * (float)((1 << BITS) - 1);
+}
+
+void resample_direct(int bits, const void *d_src, size_t pitch, int w, int h, int d, int tw, int th, int z0, int nz,
+                     const float *h_inverse, void *d_out, float *d_outf, cudaStream_t s)
+{
+    Mat M;
+    memcpy(M.m, h_inverse, sizeof(M.m));
+    dim3 grid((tw + TX - 1) / TX, (th + TY - 1) / TY, nz);
+    if (bits == 16)
+        resample_direct_kernel<unsigned short, 16><<<grid, TX * TY, 0, s>>>(
+            (const unsigned short *)d_src, w, h, d, pitch, tw, th, z0, M, (unsigned short *)d_out, d_outf);
+    else
+        resample_direct_kernel<unsigned char, 8><<<grid, TX * TY, 0, s>>>(
+            (const unsigned char *)d_src, w, h, d, pitch, tw, th, z0, M, (unsigned char *)d_out, d_outf);
+    rl_count_launch(1);
+}
+
+size_t source_pitch(int bits, int w)
+{
+    const size_t a = bits == 16 ? 8 : 16;
+    return ((size_t)w + a - 1) / a * a;
+}
+
+// transform_cuda_* (fmvd_transform.impl.cu:77-224): upload, optional mask of
+// plane td/2, resample in chunks of planes with download and file write of
+// one chunk overlapping the resampling of the next.
+void transform_file(int bits, const void *const *h_planes, int w, int h, int d, int tw, int th, int td,
+                    const float *h_inverse, const char *outfile, int masks, int border, float zspacing,
+                    const char *maskfile)
+{
+    const size_t es = bits == 16 ? 2 : 1;
+    const size_t pitch = source_pitch(bits, w);
+    void *d_src = nullptr;
+    int *d_status = nullptr;
+    if (!FMVD_CHECK(cudaMalloc(&d_src, pitch * h * d * es)) || !FMVD_CHECK(cudaMalloc(&d_status, sizeof(int))))
+        return;
+    FMVD_CHECK(cudaMemset(d_status, 0, sizeof(int)));
+    for (int z = 0; z < d; z++)
+        if (!FMVD_CHECK(cudaMemcpy2D((char *)d_src + pitch * h * z * es, pitch * es, h_planes[z], w * es, w * es, h,
+                                     cudaMemcpyHostToDevice)))
+            return;
+    cudaStream_t s;
+    FMVD_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+
+    if (masks) {
+        float *d_m = nullptr;
+        std::vector<float> hm((size_t)tw * th);
+        if (FMVD_CHECK(cudaMalloc(&d_m, sizeof(float) * tw * th)) &&
+            mask_device(d_m, td / 2, w, h, d, zspacing, tw, th, (float)border, h_inverse, s) &&
+            FMVD_CHECK(cudaMemcpyAsync(hm.data(), d_m, sizeof(float) * tw * th, cudaMemcpyDeviceToHost, s)) &&
+            FMVD_CHECK(cudaStreamSynchronize(s))) {
+            FILE *f = fopen(maskfile, "wb");
+            if (f) {
+                fwrite(hm.data(), sizeof(float), (size_t)tw * th, f);
+                fclose(f);
+            } else {
+                report_error("fmvd: could not open the mask file");
+            }
+        }
+        cudaFree(d_m);
+    }
+
+    FILE *out = fopen(outfile, "wb");
+    if (!out) {
+        report_error("fmvd: could not open the output file");
+    } else {
+        const size_t plane_bytes = (size_t)tw * th * es;
+        // The reference writes an unfilled slot ahead of the data when td < 2.
+        if (td < 2) {
+            std::vector<char> zero(plane_bytes, 0);
+            for (int i = 0; i < 2 - td; i++)
+                fwrite(zero.data(), 1, plane_bytes, out);
+        }
+        int chunk = (int)((256u << 20) / (plane_bytes ? plane_bytes : 1));
+        if (chunk < 1)
+            chunk = 1;
+        if (chunk > td)
+            chunk = td > 0 ? td : 1;
+        void *d_out[2] = {nullptr, nullptr};
+        void *h_out[2] = {nullptr, nullptr};
+        cudaEvent_t ev[2];
+        bool ok = true;
+        for (int k = 0; k < 2 && ok; k++)
+            ok = FMVD_CHECK(cudaMalloc(&d_out[k], plane_bytes * chunk)) &&
+                 FMVD_CHECK(cudaMallocHost(&h_out[k], plane_bytes * chunk)) &&
+                 FMVD_CHECK(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
+        int pending_k = -1, pending_n = 0;
+        for (int z0 = 0, k = 0; ok && z0 < td; z0 += chunk, k ^= 1) {
+            const int n = td - z0 < chunk ? td - z0 : chunk;
+            ok = resample_device(bits, d_src, pitch, w, h, d, tw, th, z0, n, h_inverse, d_out[k], nullptr, d_status,
+                                 s) &&
+                 FMVD_CHECK(cudaMemcpyAsync(h_out[k], d_out[k], plane_bytes * n, cudaMemcpyDeviceToHost, s)) &&
+                 FMVD_CHECK(cudaEventRecord(ev[k], s));
+            if (ok && pending_k >= 0) {
+                ok = FMVD_CHECK(cudaEventSynchronize(ev[pending_k]));
+                fwrite(h_out[pending_k], 1, plane_bytes * pending_n, out);
+            }
+            pending_k = k;
+            pending_n = n;
+        }
+        if (ok && pending_k >= 0) {
+            ok = FMVD_CHECK(cudaEventSynchronize(ev[pending_k]));
+            fwrite(h_out[pending_k], 1, plane_bytes * pending_n, out);
+        }
+        fclose(out);
+        for (int k = 0; k < 2; k++) {
+            cudaFree(d_out[k]);
+            cudaFreeHost(h_out[k]);
+            if (ok)
+                cudaEventDestroy(ev[k]);
+        }
+    }
+    int status = 0;
+    cudaMemcpy(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (status)
+        report_error("fmvd: a resampler brick load did not complete in time");
+    cudaStreamDestroy(s);
+    cudaFree(d_src);
+    cudaFree(d_status);
+}
+
+} // namespace fmvd

@@ -1,0 +1,71 @@
+/* Extensions of the B200 library beyond the reference API (no counterpart
+ * in bene51/gpu_deconvolution).  All return 0 on success and a non-zero code
+ * after reporting the error through the handler installed with
+ * setErrorHandler.  Stream arguments are cudaStream_t values (0 = default
+ * stream); device pointers are CUDA device memory of the current device.
+ */
+#ifndef FMVD_B200_H
+#define FMVD_B200_H
+
+#include <stddef.h>
+#include "fmvd_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- device-resident deconvolution (no datasource / datasink) ---------- */
+typedef struct fmvd_b200_plan fmvd_b200_plan;
+
+/* Same preparation as fmvd_initialize_cuda_* (kernel 2 derivation, in-place
+ * normalisation of h_Kernel, weight normalisation).  pairs_per_batch: plane
+ * pairs deconvolved together (0 = automatic, sized for L2 residency). */
+fmvd_b200_plan *fmvd_b200_plan_create(int bits, int dataH, int dataW, const float *const *h_Weights,
+                                      float **h_Kernel, int kernelH, int kernelW, fmvd_psf_type iteration_type,
+                                      int nViews, int pairs_per_batch);
+int fmvd_b200_plan_query(const fmvd_b200_plan *plan, int *fftH, int *fftW, int *pairs_per_batch);
+/* View v, plane z at d_views + (v * view_stride + z * dataH * dataW) samples;
+ * output plane z at d_out + z * dataH * dataW.  d_estimate (optional)
+ * receives nplanes float planes of fftH x fftW.  Asynchronous on stream. */
+int fmvd_b200_deconvolve_device(fmvd_b200_plan *plan, const void *d_views, size_t view_stride, void *d_out,
+                                int nplanes, int iterations, float *d_estimate, void *stream);
+void fmvd_b200_plan_destroy(fmvd_b200_plan *plan);
+
+/* Streaming plans with an explicit batch size (the fmvd_initialize_cuda_*
+ * entry points choose it automatically). */
+struct fmvd_plan_cuda_16 *fmvd_b200_initialize_cuda_16(int dataH, int dataW, float const *const *h_Weights,
+                                                       float **h_Kernel, int kernelH, int kernelW,
+                                                       fmvd_psf_type iteration_type, int nViews, int nstreams,
+                                                       datasource_16_t get_next_plane,
+                                                       datasink_16_t return_next_plane, int pairs_per_batch);
+struct fmvd_plan_cuda_8 *fmvd_b200_initialize_cuda_8(int dataH, int dataW, float const *const *h_Weights,
+                                                     float **h_Kernel, int kernelH, int kernelW,
+                                                     fmvd_psf_type iteration_type, int nViews, int nstreams,
+                                                     datasource_8_t get_next_plane, datasink_8_t return_next_plane,
+                                                     int pairs_per_batch);
+
+/* ---- resampler ---------------------------------------------------------- */
+/* Row pitch (samples) that device source volumes must use. */
+size_t fmvd_b200_source_pitch(int bits, int w);
+/* Target planes [z0, z0 + nz) from a device source volume (d planes of h
+ * rows of 'pitch' samples).  d_out: nz sample planes (or null); d_outf: nz
+ * float planes in sample units, before quantisation (or null). */
+int fmvd_b200_transform_device(int bits, const void *d_src, size_t pitch, int w, int h, int d, int tw, int th,
+                               int z0, int nz, const float *h_inverse, void *d_out, float *d_outf, void *stream);
+/* Weight mask of target plane z (tw x th floats). */
+int fmvd_b200_mask_device(float *d_out, int z, int w, int h, int d, float zspacing, int tw, int th, float border,
+                          const float *h_inverse, void *stream);
+/* transform_cuda_* into host memory: h_out receives td planes of tw x th
+ * samples (no file, no leading unfilled planes). */
+int fmvd_b200_transform_host(int bits, const void *const *h_planes, int w, int h, int d, int tw, int th, int td,
+                             const float *h_inverse, void *h_out);
+
+/* ---- instrumentation ----------------------------------------------------- */
+/* Number of kernel launches the library has issued in this process. */
+unsigned long long fmvd_b200_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FMVD_B200_H */

@@ -1,0 +1,182 @@
+"""Parity of the B200 deconvolution with the FP64 oracle and with the
+reference's own CUDA build, through the C ABI.
+
+Tolerances: float estimates within 1e-4 relative L2 of the oracle (and of the
+reference build) after every tested iteration count; sample outputs within
+one unit of the oracle (truncation of values that differ in the last float
+bits), and identical in almost every voxel.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from gpu_deconvolution_b200 import api, synth
+from oracle import fmvd_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-4
+
+
+def device_estimates(views, weights, kernels, psf, iterations, pairs=0):
+    import torch
+    V, D, H, W = views.shape
+    plan = api.DevicePlan(H, W, weights, [k.copy() for k in kernels], psf, bits=16 if views.dtype == np.uint16 else 8,
+                          pairs_per_batch=pairs)
+    tv = torch.from_numpy(np.ascontiguousarray(views).view(np.uint8).reshape(-1)).cuda()
+    out = torch.zeros(D * H * W * views.dtype.itemsize, dtype=torch.uint8, device="cuda")
+    est = torch.zeros((D, plan.fftH, plan.fftW), dtype=torch.float32, device="cuda")
+    plan.run(tv, out, iterations, est, nplanes=D)
+    torch.cuda.synchronize()
+    res = out.cpu().numpy().view(views.dtype).reshape(D, H, W), est.cpu().numpy()
+    plan.destroy()
+    return res
+
+
+def oracle_estimates(views, weights, kernels, psf, iterations):
+    out, est = O.deconvolve_volume(views, list(weights), list(kernels), psf, iterations,
+                                   bits=16 if views.dtype == np.uint16 else 8, return_float=True)
+    return out, est
+
+
+def check_outputs(out, ref_out):
+    d = np.abs(out.astype(np.int64) - ref_out.astype(np.int64))
+    assert d.max() <= 1, d.max()
+    assert (d > 0).mean() < 1e-2
+
+
+@pytest.mark.parametrize("iterations", [1, 2, 5])
+def test_small_two_views_vs_oracle(iterations):
+    views, psfs, weights, _ = synth.plain_rl_views(shape=(3, 40, 48), n_views=2, n_beads=12, ksize=9,
+                                                  sigma=(1.2, 2.5), seed=3)
+    out, est = device_estimates(views, weights, psfs, 0, iterations)
+    oout, oest = oracle_estimates(views, weights, psfs, 0, iterations)
+    assert rel_l2(est, oest) < TOL
+    check_outputs(out, oout)
+
+
+@pytest.mark.parametrize("psf", [1, 2, 3])
+def test_psf_types_vs_oracle(psf):
+    views, psfs, _, _ = synth.plain_rl_views(shape=(2, 36, 36), n_views=3, n_beads=10, ksize=7, sigma=(1.0, 2.0),
+                                            seed=4)
+    rng = np.random.default_rng(5)
+    weights = [rng.uniform(0.1, 1.0, (36, 36)).astype(np.float32) for _ in range(3)]
+    out, est = device_estimates(views, weights, psfs, psf, 3)
+    oout, oest = oracle_estimates(views, weights, psfs, psf, 3)
+    assert rel_l2(est, oest) < TOL
+    check_outputs(out, oout)
+
+
+def test_eight_bit_vs_oracle():
+    views, psfs, weights, _ = synth.plain_rl_views(shape=(3, 33, 37), n_views=2, n_beads=8, ksize=7, seed=6, bits=8)
+    out, est = device_estimates(views, weights, psfs, 0, 3)
+    oout, oest = oracle_estimates(views, weights, psfs, 0, 3)
+    assert rel_l2(est, oest) < TOL
+    check_outputs(out, oout)
+
+
+def test_nonsquare_kernel_borders():
+    rng = np.random.default_rng(13)
+    gt = synth.bead_volume((2, 30, 50), 10, rng)
+    kns = [synth.gaussian_psf(5, 11, 2.0, 1.0, 0.0), synth.gaussian_psf(5, 11, 1.0, 1.5, 30.0)]
+    views = np.stack([synth.quantise(synth.blur_planes(gt, k), rng) for k in kns])
+    w = [np.ones((30, 50), np.float32)] * 2
+    out, est = device_estimates(views, w, kns, 0, 2)
+    oout, oest = oracle_estimates(views, w, kns, 0, 2)
+    assert rel_l2(est, oest) < TOL
+    check_outputs(out, oout)
+
+
+# every supported FFT length, in the row role and in the column role
+LENGTH_PAIRS = [(16, 4096), (32, 3584), (64, 3072), (128, 2560), (256, 2048), (512, 1536), (1024, 1024),
+                (4096, 16), (3584, 32), (3072, 64), (2560, 128), (2048, 256), (1536, 512)]
+
+
+@pytest.mark.parametrize("fh,fw", LENGTH_PAIRS)
+def test_every_fft_length(fh, fw):
+    k = 5
+    H, W = fh - k + 1, fw - k + 1
+    rng = np.random.default_rng(fh * 7 + fw)
+    views = rng.integers(50, 3000, (1, 2, H, W)).astype(np.uint16)
+    psf = [synth.gaussian_psf(k, k, 1.0, 1.6, 20.0)]
+    w = [np.ones((H, W), np.float32)]
+    out, est = device_estimates(views, w, psf, 0, 1)
+    assert est.shape[1:] == (fh, fw)
+    oout, oest = oracle_estimates(views, w, psf, 0, 1)
+    assert rel_l2(est, oest) < TOL
+    check_outputs(out, oout)
+
+
+def test_config_plane_512_vs_oracle():
+    """The plain-RL workload's plane geometry (256^2 data, 17^2 kernels -> 512^2)."""
+    views, psfs, weights, _ = synth.plain_rl_views(shape=(2, 256, 256), n_views=2, n_beads=40, ksize=17, seed=8)
+    out, est = device_estimates(views, weights, psfs, 0, 3)
+    oout, oest = oracle_estimates(views, weights, psfs, 0, 3)
+    assert est.shape[1:] == (512, 512)
+    assert rel_l2(est, oest) < TOL
+    check_outputs(out, oout)
+
+
+def test_batching_is_invisible():
+    """Batch size changes only the schedule: results are bitwise identical."""
+    views, psfs, weights, _ = synth.plain_rl_views(shape=(7, 40, 40), n_views=2, n_beads=10, ksize=9, seed=9)
+    a, ea = device_estimates(views, weights, psfs, 0, 2, pairs=1)
+    b, eb = device_estimates(views, weights, psfs, 0, 2, pairs=8)
+    assert np.array_equal(a, b)
+    assert np.array_equal(ea, eb)
+
+
+def test_zero_iterations_returns_initial_estimate():
+    views, psfs, weights, _ = synth.plain_rl_views(shape=(2, 20, 20), n_views=3, n_beads=4, ksize=5, seed=10)
+    out, est = device_estimates(views, weights, psfs, 0, 0)
+    assert np.all(out == 30)
+    assert np.allclose(est, 30.0)
+
+
+def test_streaming_api_matches_device_api():
+    views, psfs, weights, _ = synth.plain_rl_views(shape=(5, 40, 44), n_views=2, n_beads=10, ksize=9, seed=12)
+    dev, _ = device_estimates(views, weights, psfs, 0, 3)
+    got, stats = api.deconvolve(views, weights, psfs, 0, 3, nstreams=3, pairs_per_batch=1, return_stats=True)
+    assert np.array_equal(got, dev)
+    assert stats["source_calls"] == 6 and stats["sink_calls"] == 5
+
+
+def test_streaming_fewer_planes_than_streams():
+    """Reference quirk: a source with 1 plane and nstreams = 3 gives 3 sink
+    calls and 4 source calls; the first plane is the real result."""
+    views, psfs, weights, _ = synth.plain_rl_views(shape=(1, 24, 24), n_views=2, n_beads=4, ksize=5, seed=13)
+    got, stats = api.deconvolve(views, weights, psfs, 0, 2, nstreams=3, return_stats=True)
+    assert stats["source_calls"] == 4 and stats["sink_calls"] == 3
+    oout, _ = oracle_estimates(views, weights, psfs, 0, 2)
+    check_outputs(got[:1], oout)
+
+
+def test_kernels_normalised_in_place(lib):
+    """The caller's kernels come back normalised (fmvd_deconvolve.impl.cpp:63-64)."""
+    psf = synth.gaussian_psf(7, 7, 1.0, 2.0, 0.0) * 5.0
+    ks = [psf.copy(), (psf * 3).copy()]
+    plan = api.StreamingPlan(20, 20, [np.ones((20, 20), np.float32)] * 2, ks, 0, 3)
+    for k in plan.kernels:
+        assert abs(float(k.astype(np.float64).sum()) - 1.0) < 1e-5
+    plan.destroy()
+
+
+def test_files_entry_point(tmp_path):
+    views, psfs, weights, _ = synth.plain_rl_views(shape=(4, 30, 34), n_views=2, n_beads=6, ksize=7, seed=14)
+    paths = []
+    for v in range(2):
+        p = tmp_path / f"v{v}.raw"
+        views[v].tofile(p)
+        paths.append(str(p))
+    outp = str(tmp_path / "out.raw")
+    api.deconvolve_files(paths, outp, 34, 30, 4, weights, [k.copy() for k in psfs], 0, 2)
+    got = np.fromfile(outp, np.uint16).reshape(-1, 30, 34)
+    oout, _ = oracle_estimates(views, weights, psfs, 0, 2)
+    assert got.shape[0] == 4
+    check_outputs(got, oout)
+
+
+def test_unsupported_size_reports_error():
+    from gpu_deconvolution_b200.native import FmvdError
+    with pytest.raises(FmvdError):
+        api.DevicePlan(5000, 64, [np.ones((5000, 64), np.float32)], [np.ones((3, 3), np.float32)], 0)
