@@ -1,0 +1,434 @@
+#!/usr/bin/env python
+"""Benchmark of the multi-view reconstruction path on B200.
+
+Workload (the transform + plain-RL configuration): 4 raw views, uint16
+512 x 512 x 128 with z spacing 3 (seeded synthetic beads and shells, blurred
+per plane, Poisson noise); inverse affines = rotation about y by
+0/90/180/270 degrees, z scale 3, shift U[-8, 8]; trilinear resampling of each
+view into a 512 x 512 x 384 common frame (uint16, as the reference API
+produces); weights = the transformed masks (border 16); then 20 plane-wise
+RL iterations with 31 x 31 anisotropic Gaussian kernels (sigma 1.2 x 5.0,
+rotated per view), FP32.  A step is one such volume: resample all views and
+deconvolve all 384 planes.
+
+Metric: RL voxel-iter/s = 512 * 512 * 384 frame voxels * 20 iterations /
+step time.  'value' is measured with inputs resident in device memory (CUDA
+events on the launch stream); 'e2e' through the C ABI with host buffers
+(transform_host, then fmvd_initialize / deconvolve_planes / destroy with a
+datasource and datasink on host memory).  Inputs (268 MB of source views)
+exceed the 126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank deconvolves its own
+volume (weak scaling); the time is the maximum over ranks.  --impl reference
+times the reference's own implementation of the path: the reference CUDA
+library built from the upstream sources (cuFFT) for the deconvolution and the
+texture-unit restatement of its resampler, through their host-memory API.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+V = 4
+SRC = (128, 512, 512)     # d, h, w of each raw view
+FRAME = (384, 512, 512)   # td, th, tw
+ITERATIONS = 20
+KSIZE = 31
+ZSCALE = 3.0
+BORDER = 16
+BYTES_PER_PADDED_VOXEL_VIEW_ITER = 14  # read e (4) + write e (4) + data (2) + weight (4)
+METRIC = "RL voxel-iter/s"
+UNIT = "voxel-iter/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--small", action="store_true", help="small volume for profiler captures")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------ data
+def workload(seed: int, small: bool):
+    """Seeded synthetic views, matrices and kernels (numpy + torch on the GPU
+    for the blur; data generation only)."""
+    import torch
+    from gpu_deconvolution_b200 import synth
+    src = (SRC[0] // 8, SRC[1], SRC[2]) if small else SRC
+    frame = (FRAME[0] // 8, FRAME[1], FRAME[2]) if small else FRAME
+    rng = np.random.default_rng(seed)
+    gt = synth.bead_volume(src, 2000 if not small else 250, rng, shells=3)
+    psfs = [synth.gaussian_psf(KSIZE, KSIZE, 1.2, 5.0, 180.0 * v / V) for v in range(V)]
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    vols = []
+    gtt = torch.from_numpy(gt).cuda()
+    d, h, w = src
+    for v in range(V):
+        k = torch.from_numpy(psfs[v]).cuda()
+        fh, fw = h + KSIZE - 1, w + KSIZE - 1
+        spec = torch.fft.rfft2(k, s=(fh, fw))
+        out = torch.empty_like(gtt)
+        for z0 in range(0, d, 32):
+            blk = torch.fft.irfft2(torch.fft.rfft2(gtt[z0:z0 + 32], s=(fh, fw)) * spec, s=(fh, fw))
+            out[z0:z0 + 32] = blk[:, KSIZE // 2:KSIZE // 2 + h, KSIZE // 2:KSIZE // 2 + w]
+        noisy = torch.poisson(out.clamp_min(0), generator=g)
+        vols.append(noisy.clamp(0, 65535).round().to(torch.int32).cpu().numpy().astype(np.uint16))
+    shifts = rng.uniform(-8, 8, (V, 3))
+    mats = [synth.rotation_y_inverse(90.0 * v, frame, src, ZSCALE, shifts[v]) for v in range(V)]
+    return vols, mats, psfs, src, frame
+
+
+def masks_for(mats, src, frame):
+    import torch
+    from gpu_deconvolution_b200 import api
+    out = []
+    for m in mats:
+        t = torch.zeros((frame[1], frame[2]), dtype=torch.float32, device="cuda")
+        api.mask_device(t, frame[0] // 2, src[2], src[1], src[0], ZSCALE, frame[2], frame[1], BORDER, m)
+        torch.cuda.synchronize()
+        out.append(t.cpu().numpy().astype(np.float32))
+    return out
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling during the timed region (200 ms period)."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------- utilities
+def peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """Per view-update DRAM bytes of the RL passes from the committed ncu
+    summary, if one exists."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "rl_passes_traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def dist_setup(n):
+    import torch
+    if n <= 1 or "WORLD_SIZE" not in os.environ:
+        return 0, 1, 0
+    import datetime
+    import torch.distributed as dist
+    rank = int(os.environ["RANK"])
+    world = int(os.environ["WORLD_SIZE"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier_max(t, world):
+    import torch
+    if world <= 1:
+        return t
+    import torch.distributed as dist
+    x = torch.tensor([t], dtype=torch.float64, device="cuda")
+    dist.all_reduce(x, op=dist.ReduceOp.MAX)
+    return float(x.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# --------------------------------------------------------- CPU baseline
+def cpu_baseline(vols, weights, psfs):
+    """The C/OpenMP port of the per-plane update (oracle/fmvd_cpu.c) on a
+    bounded sample: one plane pair per host thread, 4 iterations, all views,
+    on the same 512 x 512 plane geometry."""
+    import ctypes as C
+    from oracle import fmvd_oracle as O
+    path = os.path.join(ROOT, "oracle", "_build", "libfmvd_cpu.so")
+    if not os.path.exists(path):
+        return None
+    lib = C.CDLL(path)
+    threads = int(lib.fmvdcpu_max_threads())
+    planes = min(2 * threads, 96)
+    its = 4
+    H, W = FRAME[1], FRAME[2]
+    sample = np.ascontiguousarray(np.stack([v[:planes, :H, :W] if v.shape[0] >= planes else
+                                            np.resize(v, (planes, H, W)) for v in vols]))
+    k1 = np.stack([O.normalize(p) for p in psfs]).astype(np.float32)
+    k2 = np.stack(O.compute_kernel2(psfs, 0)).astype(np.float32)
+    w = np.ascontiguousarray(np.stack(weights).astype(np.float32))
+    out = np.zeros((planes, H, W), np.uint16)
+    P = lambda a: C.c_void_p(a.ctypes.data)
+    t0 = time.perf_counter()
+    lib.fmvdcpu_deconvolve(16, P(sample), P(w), P(k1), P(k2), V, planes, H, W, KSIZE, KSIZE, its, P(out), None,
+                           threads)
+    dt = time.perf_counter() - t0
+    return {"value": H * W * planes * its / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"C/OpenMP port of the per-plane update, {planes} planes x {its} iterations x {V} views "
+                      f"at 512x512 (1024x1024 padded), {dt:.1f} s"}
+
+
+# ---------------------------------------------------------------- B200
+def run_b200(args):
+    import torch
+    from gpu_deconvolution_b200 import api, native
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    lib = native.load()
+    vols, mats, psfs, src, frame = workload(1234 + rank, args.small)
+    weights = masks_for(mats, src, frame)
+    d, h, w = src
+    td, th, tw = frame
+    pitch = api.source_pitch(16, w)
+    src_dev = torch.zeros((V, d, h, pitch), dtype=torch.int16, device="cuda")
+    for v in range(V):
+        src_dev[v, :, :, :w] = torch.from_numpy(vols[v].view(np.int16)).cuda()
+    frame_dev = torch.zeros((V, td, th, tw), dtype=torch.int16, device="cuda")
+    out_dev = torch.zeros((td, th, tw), dtype=torch.int16, device="cuda")
+    plan = api.DevicePlan(th, tw, weights, [p.copy() for p in psfs], 0, bits=16)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def step(ev=None):
+        for v in range(V):
+            api.transform_device(src_dev[v], pitch, w, h, d, mats[v], tw, th, 0, td, out=frame_dev[v], stream=stream)
+        if ev:
+            ev[0].record()
+        plan.run(frame_dev, out_dev, ITERATIONS, stream=stream)
+        if ev:
+            ev[1].record()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = lib.fmvd_b200_launch_count()
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    rl_events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                 for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        e_start.record()
+        for i in range(args.steps):
+            step(rl_events[i])
+        e_end.record()
+        torch.cuda.synchronize()
+    launches = lib.fmvd_b200_launch_count() - launches0
+    t_total = e_start.elapsed_time(e_end) / 1e3
+    t_rl = sum(a.elapsed_time(b) for a, b in rl_events) / 1e3
+    barrier(world)
+    t_max = barrier_max(t_total, world)
+    voxel_iters = td * th * tw * ITERATIONS
+    value = voxel_iters * args.steps * world / t_max
+
+    # roofline of the fused RL passes (algorithmic bytes per padded voxel, view and iteration)
+    H, W = plan.fftH, plan.fftW
+    alg_bytes = BYTES_PER_PADDED_VOXEL_VIEW_ITER * H * W * td * V * ITERATIONS * args.steps
+    achieved = alg_bytes / t_rl / 1e9
+    peak, peak_kind = peak_hbm()
+    traffic = profiled_traffic()
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, vols, mats, psfs, weights, src, frame)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        frames = frame_dev[:, :min(96, td)].cpu().numpy().view(np.uint16)
+        cpu = cpu_baseline(list(frames), weights, psfs)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "transform + plain RL: 4 views u16 512x512x128 (z spacing 3) -> 512x512x384 "
+                                   "frame, 20 RL iterations, 31x31 PSFs, FFT plane 1024x1024" +
+                                   (" [small]" if args.small else ""),
+                       "views": V, "frame": list(frame), "iterations": ITERATIONS, "fft_plane": [H, W],
+                       "pairs_per_batch": plan.pairs_per_batch,
+                       "l2": "inputs larger than L2 (268 MB of source views per step)",
+                       "rl_ms_per_step": t_rl / args.steps * 1e3,
+                       "transform_ms_per_step": (t_total - t_rl) / args.steps * 1e3},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "kernel": "fused RL view update (row divide, column K^, row update, column K passes)",
+                         "algorithmic_bytes": "14 B per padded voxel per view per iteration",
+                         "traffic": (traffic or {}).get("bytes_per_view_update_per_padded_voxel")},
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    plan.destroy()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_e2e(args, vols, mats, psfs, weights, src, frame):
+    """The same step through the C ABI with host buffers (pinned sources)."""
+    import torch
+    from gpu_deconvolution_b200 import api
+    td, th, tw = frame
+    pinned = [torch.from_numpy(v.view(np.int16)).pin_memory().numpy().view(np.uint16) for v in vols]
+
+    def step():
+        frames = np.stack([api.transform_host(pinned[v], mats[v], tw, th, td) for v in range(V)])
+        return api.deconvolve(frames, weights, [p.copy() for p in psfs], 0, ITERATIONS, nstreams=3)
+
+    step()
+    t0 = time.perf_counter()
+    n = max(1, min(args.steps, 2))
+    for _ in range(n):
+        out = step()
+    dt = (time.perf_counter() - t0) / n
+    d = src[0]
+    h2d = V * d * src[1] * src[2] * 2 + V * td * th * tw * 2
+    d2h = V * td * th * tw * 2 + td * th * tw * 2
+    assert out.shape[0] == td
+    return {"value": td * th * tw * ITERATIONS / dt, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": dt * 1e3,
+            "api": "fmvd_b200_transform_host x4 + fmvd_initialize/deconvolve_planes/destroy_cuda_16"}
+
+
+# ------------------------------------------------------------ reference
+def run_reference(args):
+    import ctypes as C
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    ref = os.path.join(ROOT, "oracle", "_ref", "libfmvd_ref.so")
+    tex_path = os.path.join(ROOT, "oracle", "_ref", "libfmvd_reftex.so")
+    if not (os.path.exists(ref) and os.path.exists(tex_path)):
+        print(json.dumps({"impl": "reference", "unavailable": "reference build (oracle/_ref) not present"}))
+        return
+    import torch
+    torch.cuda.set_device(0)
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_golden
+    lib, tex = make_golden.load_ref()
+    vols, mats, psfs, src, frame = workload(1234, args.small)
+    weights = masks_for(mats, src, frame)
+    d, h, w = src
+    td, th, tw = frame
+
+    def step():
+        frames = np.zeros((V, td, th, tw), np.uint16)
+        for v in range(V):
+            m = np.ascontiguousarray(mats[v])
+            r = tex.reftex_transform(16, np.ascontiguousarray(vols[v]).ctypes.data, w, h, d, tw, th, td,
+                                     m.ctypes.data, frames[v].ctypes.data, None, None)
+            assert r == 0
+        res = make_golden.ref_deconvolve(lib, frames, weights, [p.copy() for p in psfs], 0, ITERATIONS, 3, False)
+        return res["out"]
+
+    for _ in range(min(args.warmup, 1)):
+        step()
+    t0 = time.perf_counter()
+    n = max(1, min(args.steps, 2))
+    for _ in range(n):
+        step()
+    dt = (time.perf_counter() - t0) / n
+    value = td * th * tw * ITERATIONS / dt
+    h2d = V * d * h * w * 2 + V * td * th * tw * 2
+    d2h = V * td * th * tw * 2 + td * th * tw * 2
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": 1, "steps": n,
+        "warmup": min(args.warmup, 1), "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "transform + plain RL: 4 views u16 512x512x128 (z spacing 3) -> 512x512x384 frame, "
+                               "20 RL iterations, 31x31 PSFs, FFT plane 1024x1024" + (" [small]" if args.small else ""),
+                   "views": V, "frame": list(frame), "iterations": ITERATIONS},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 0, "kind": "reference",
+                         "sample": "the reference's own implementation, which is CUDA: upstream deconvolution "
+                                   "sources built for sm_100a with cuFFT (nstreams 3) and the texture-unit "
+                                   "restatement of its resampler, host buffers in and out, on 1 B200"},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -130,6 +130,23 @@ std::vector<double2> twiddles_d(int n)
     return t;
 }
 
+// Twiddles of the warp FFT's four-step split N = T x E: [k1 * T + t] =
+// exp(-2 pi i t k1 / N) for t < T, k1 < E (zeros when N has no warp split).
+std::vector<float2> warp_twiddles(int n)
+{
+    std::vector<float2> t(n, make_float2(0.f, 0.f));
+    const int T = rl_warp_lanes(n);
+    if (T == 0)
+        return t;
+    const int E = n / T;
+    for (int k1 = 0; k1 < E; k1++)
+        for (int l = 0; l < T; l++) {
+            const double a = -2.0 * M_PI * (double)((long long)l * k1 % n) / (double)n;
+            t[k1 * T + l] = make_float2((float)cos(a), (float)sin(a));
+        }
+    return t;
+}
+
 unsigned g_constants_uploaded = 0;
 
 } // namespace
@@ -208,7 +225,8 @@ Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weig
               FMVD_CHECK(cudaMalloc(&e->weights, sizeof(float) * plane * nViews)) &&
               FMVD_CHECK(cudaMalloc(&e->C, sizeof(float2) * (size_t)H * W * e->pairs_cap)) &&
               FMVD_CHECK(cudaMalloc(&e->est, sizeof(float2) * (size_t)H * W * e->pairs_cap)) &&
-              FMVD_CHECK(cudaMalloc(&e->twH, sizeof(float2) * H)) && FMVD_CHECK(cudaMalloc(&e->twW, sizeof(float2) * W));
+              FMVD_CHECK(cudaMalloc(&e->twH, sizeof(float2) * H)) && FMVD_CHECK(cudaMalloc(&e->twW, sizeof(float2) * W)) &&
+              FMVD_CHECK(cudaMalloc(&e->wtwH, sizeof(float2) * H)) && FMVD_CHECK(cudaMalloc(&e->wtwW, sizeof(float2) * W));
     if (!ok) {
         engine_destroy(e);
         return nullptr;
@@ -222,8 +240,11 @@ Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weig
             fH[i] = make_float2((float)tH[i].x, (float)tH[i].y);
         for (int i = 0; i < W; i++)
             fW[i] = make_float2((float)tW[i].x, (float)tW[i].y);
+        std::vector<float2> wH = warp_twiddles(H), wW = warp_twiddles(W);
         ok = FMVD_CHECK(cudaMemcpy(e->twH, fH.data(), sizeof(float2) * H, cudaMemcpyHostToDevice)) &&
-             FMVD_CHECK(cudaMemcpy(e->twW, fW.data(), sizeof(float2) * W, cudaMemcpyHostToDevice));
+             FMVD_CHECK(cudaMemcpy(e->twW, fW.data(), sizeof(float2) * W, cudaMemcpyHostToDevice)) &&
+             FMVD_CHECK(cudaMemcpy(e->wtwH, wH.data(), sizeof(float2) * H, cudaMemcpyHostToDevice)) &&
+             FMVD_CHECK(cudaMemcpy(e->wtwW, wW.data(), sizeof(float2) * W, cudaMemcpyHostToDevice));
 
         // kernel spectra
         double2 *d_twH = nullptr, *d_twW = nullptr, *work = nullptr;
@@ -280,6 +301,8 @@ void engine_destroy(Engine *e)
     cudaFree(e->est);
     cudaFree(e->twH);
     cudaFree(e->twW);
+    cudaFree(e->wtwH);
+    cudaFree(e->wtwW);
     delete e;
 }
 
@@ -298,7 +321,7 @@ void engine_batch(Engine *e, const void *data, size_t view_stride, void *out, in
     b.npairs = (nplanes + 1) / 2;
     b.nplanes = nplanes;
     b.init_value = 10.0f * (float)V;  // fmvd_deconvolve_cuda.impl.cu:62, once per view
-    RlTables t{e->twH, e->twW};
+    RlTables t{e->twH, e->twW, e->wtwH, e->wtwW};
     const float2 *spec = e->spec;
     const size_t se = e->spec_elems;
 

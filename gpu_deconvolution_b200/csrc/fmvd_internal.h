@@ -33,7 +33,8 @@ struct Engine {
     float *weights;         // V x dataH x dataW normalised weights
     float2 *C;              // pairs_cap x H x W
     float2 *est;            // pairs_cap x H x W
-    float2 *twH, *twW;
+    float2 *twH, *twW;      // exp(-2 pi i n / N), block engine
+    float2 *wtwH, *wtwW;    // warp engine: [k1 * T + t] = exp(-2 pi i t k1 / N)
 };
 
 // Build an engine.  h_Kernel is normalised in place (reference semantics).

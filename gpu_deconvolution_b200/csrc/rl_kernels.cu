@@ -24,6 +24,7 @@
 // resident in L2.
 #include "fft_engine.cuh"
 #include "rl_kernels.h"
+#include "warp_fft.cuh"
 
 #include <math.h>
 #include <stdint.h>
@@ -37,14 +38,10 @@ static unsigned long long g_launches = 0;
 unsigned long long rl_launch_count() { return g_launches; }
 void rl_count_launch(unsigned long long n) { g_launches += n; }
 
-// Work-plane tiling: 2 rows x 8 columns of complex (128 bytes) per tile.
-constexpr int kTR = 2;
-constexpr int kTC = 8;
-
-__host__ __device__ __forceinline__ size_t tile_index(int y, int x, int W)
-{
-    return (size_t)(y >> 1) * (2 * W) + (size_t)(x >> 3) * 16 + (y & 1) * 8 + (x & 7);
-}
+// Work planes are row-major (natural order): element (y, x) of pair p at
+// C[(p * H + y) * W + x].  Column blocks read runs of 4 to 8 complex values
+// (32 to 64 bytes, whole L2 sectors) per row.
+__host__ __device__ __forceinline__ size_t tile_index(int y, int x, int W) { return (size_t)y * W + x; }
 
 __device__ __forceinline__ int clamp_src(int i, int n, int border)
 {
@@ -83,9 +80,7 @@ __device__ __forceinline__ void load_rows(const float2 *__restrict__ src, float 
 #pragma unroll 4
     for (int u = threadIdx.x; u < units; u += NT) {
         const int l = 2 * u;
-        const int yl2 = l / (2 * W), rem = l % (2 * W);
-        const int yl = 2 * yl2 + ((rem & 15) >> 3);
-        const int x = (rem >> 4) * 8 + (rem & 7);
+        const int yl = l / W, x = l % W;
         const float4 q = s4[u];
         const int a = L::at(yl, x);
         sre[a] = q.x;
@@ -106,9 +101,7 @@ __device__ __forceinline__ void store_rows(float2 *__restrict__ dst, const float
 #pragma unroll 4
     for (int u = threadIdx.x; u < units; u += NT) {
         const int l = 2 * u;
-        const int yl2 = l / (2 * W), rem = l % (2 * W);
-        const int yl = 2 * yl2 + ((rem & 15) >> 3);
-        const int x = (rem >> 4) * 8 + (rem & 7);
+        const int yl = l / W, x = l % W;
         const int a = L::at(yl, x), a1 = L::at(yl, x + 1);
         d4[u] = make_float4(sre[a], sim[a], sre[a1], sim[a1]);
     }
@@ -133,6 +126,86 @@ __device__ __forceinline__ void store_sample(void *base, size_t idx, float v, in
     }
 }
 
+// Element-wise work of the row passes on row y of pair p (row-invariant
+// pointers computed once):
+//   INIT:   estimate = 10 * nViews (imaginary part 0 for a missing second plane)
+//   DIVIDE: blur b -> data / b where b > 1, else b (divide_kernel, the
+//           reference's in-place quirk)
+//   UPDATE: correction r -> e + w (e r - e) (multiply32_kernel); after the
+//           last view of the last iteration also the output samples
+template <int MODE>
+struct RowWork {
+    const RlDims &d;
+    float2 *est;            // row y of the pair's estimate
+    const void *src0, *src1; // data rows (clamped) of planes 2p and 2p+1, view a.view
+    const float *wrow;      // weight row (clamped)
+    void *out0, *out1;      // output rows, or null
+    bool has1;
+    float init0, init1;
+
+    __device__ __forceinline__ RowWork(const RowArgs &a, int p, int y) : d(a.d)
+    {
+        const int W = d.W;
+        has1 = 2 * p + 1 < a.b.nplanes;
+        est = a.b.est + ((size_t)p * d.H + y) * W;
+        init0 = a.b.init_value;
+        init1 = has1 ? a.b.init_value : 0.f;
+        const size_t es = d.bits == 16 ? 2 : 1;
+        src0 = src1 = nullptr;
+        wrow = nullptr;
+        out0 = out1 = nullptr;
+        if (MODE == ROW_DIVIDE) {
+            const size_t base = (size_t)a.view * a.b.view_stride + (size_t)clamp_src(y, d.dataH, d.byD) * d.dataW;
+            src0 = (const char *)a.b.data + (base + (size_t)(2 * p) * a.b.plane_stride) * es;
+            src1 = has1 ? (const char *)a.b.data + (base + (size_t)(2 * p + 1) * a.b.plane_stride) * es : src0;
+        }
+        if (MODE == ROW_UPDATE) {
+            wrow = a.b.weights + (size_t)a.view * d.dataH * d.dataW + (size_t)clamp_src(y, d.dataH, d.byW) * d.dataW;
+            if (a.last && y < d.dataH) {
+                out0 = (char *)a.b.out + ((size_t)(2 * p) * a.b.plane_stride + (size_t)y * d.dataW) * es;
+                if (has1)
+                    out1 = (char *)a.b.out + ((size_t)(2 * p + 1) * a.b.plane_stride + (size_t)y * d.dataW) * es;
+            }
+        }
+    }
+
+    __device__ __forceinline__ void apply(int x, float2 &v) const
+    {
+        if (MODE == ROW_INIT) {
+            v = make_float2(init0, init1);
+            est[x] = v;
+        } else if (MODE == ROW_DIVIDE) {
+            const int sx = clamp_src(x, d.dataW, d.bxD);
+            float2 q = v;
+            if (q.x > 1.f)
+                q.x = load_sample(src0, sx, d.bits) / q.x;
+            if (q.y > 1.f)
+                q.y = has1 ? load_sample(src1, sx, d.bits) / q.y : 0.f;
+            v = q;
+        } else {
+            const float w = __ldg(wrow + clamp_src(x, d.dataW, d.bxW));
+            float2 c = est[x];
+            const float2 r = v;
+            c.x += w * (c.x * r.x - c.x);
+            c.y += w * (c.y * r.y - c.y);
+            est[x] = c;
+            v = c;
+            if (out0 && x < d.dataW) {
+                store_sample(out0, x, c.x, d.bits);
+                if (out1)
+                    store_sample(out1, x, c.y, d.bits);
+            }
+        }
+    }
+};
+
+template <int MODE>
+__device__ __forceinline__ void pointwise(const RowArgs &a, int p, int y, int x, float2 &v)
+{
+    RowWork<MODE>(a, p, y).apply(x, v);
+}
+
+// Row pass for W > 1024: F rows per block through the shared-memory Stockham engine.
 template <int W, int F, int MODE>
 __global__ void __launch_bounds__(Cfg<W, F>::NT) row_pass(const RowArgs a)
 {
@@ -141,11 +214,9 @@ __global__ void __launch_bounds__(Cfg<W, F>::NT) row_pass(const RowArgs a)
     float *sim = smem + SmemLayout<W>::floats(F);
     constexpr int NT = Cfg<W, F>::NT;
     using EG = Edge<W, F, NT>;
-    const RlDims &d = a.d;
     const int p = blockIdx.y;
     const int y0 = blockIdx.x * F;
-    const int H = d.H;
-    float2 *C = a.b.C + (size_t)p * H * W + (size_t)y0 * W;
+    float2 *C = a.b.C + (size_t)p * a.d.H * W + (size_t)y0 * W;
     float2 v[EG::E];
 
     if (MODE != ROW_INIT) {
@@ -153,67 +224,67 @@ __global__ void __launch_bounds__(Cfg<W, F>::NT) row_pass(const RowArgs a)
         __syncthreads();
         fft<W, F, NT, +1, false>(sre, sim, v, a.tw);
     }
-
-    const int z0 = 2 * p, z1 = 2 * p + 1;
-    const bool has1 = z1 < a.b.nplanes;
-    float2 *est = a.b.est + (size_t)p * H * W;
-
-    if (MODE == ROW_INIT) {
-        const float e0 = a.b.init_value, e1 = has1 ? a.b.init_value : 0.f;
 #pragma unroll
-        for (int e = 0; e < EG::E; e++) {
-            int f, x;
-            EG::pos(e, f, x);
-            v[e] = make_float2(e0, e1);
-            est[(size_t)(y0 + f) * W + x] = v[e];
-        }
-    } else if (MODE == ROW_DIVIDE) {
-        const size_t vb = (size_t)a.view * a.b.view_stride;
-        const size_t o0 = vb + (size_t)z0 * a.b.plane_stride;
-        const size_t o1 = vb + (size_t)(has1 ? z1 : z0) * a.b.plane_stride;
-#pragma unroll
-        for (int e = 0; e < EG::E; e++) {
-            int f, x;
-            EG::pos(e, f, x);
-            const int sy = clamp_src(y0 + f, d.dataH, d.byD);
-            const int sx = clamp_src(x, d.dataW, d.bxD);
-            const size_t si = (size_t)sy * d.dataW + sx;
-            float2 q = v[e];
-            if (q.x > 1.f)
-                q.x = load_sample(a.b.data, o0 + si, d.bits) / q.x;
-            if (q.y > 1.f)
-                q.y = has1 ? load_sample(a.b.data, o1 + si, d.bits) / q.y : 0.f;
-            v[e] = q;
-        }
-    } else {  // ROW_UPDATE
-        const float *wv = a.b.weights + (size_t)a.view * d.dataH * d.dataW;
-#pragma unroll
-        for (int e = 0; e < EG::E; e++) {
-            int f, x;
-            EG::pos(e, f, x);
-            const int y = y0 + f;
-            const float w = __ldg(wv + (size_t)clamp_src(y, d.dataH, d.byW) * d.dataW + clamp_src(x, d.dataW, d.bxW));
-            const size_t ei = (size_t)y * W + x;
-            float2 c = est[ei];
-            const float2 r = v[e];
-            c.x += w * (c.x * r.x - c.x);
-            c.y += w * (c.y * r.y - c.y);
-            est[ei] = c;
-            v[e] = c;
-            if (a.last && y < d.dataH && x < d.dataW) {
-                store_sample(a.b.out, (size_t)z0 * a.b.plane_stride + (size_t)y * d.dataW + x, c.x, d.bits);
-                if (has1)
-                    store_sample(a.b.out, (size_t)z1 * a.b.plane_stride + (size_t)y * d.dataW + x, c.y, d.bits);
-            }
-        }
-        if (a.last)
-            return;
+    for (int e = 0; e < EG::E; e++) {
+        int f, x;
+        EG::pos(e, f, x);
+        pointwise<MODE>(a, p, y0 + f, x, v[e]);
     }
-
+    if (MODE == ROW_UPDATE && a.last)
+        return;
     fft<W, F, NT, -1, true>(sre, sim, v, a.tw);
     regs_to_smem<W, F, NT>(sre, sim, v);
     __syncthreads();
     store_rows<W, F>(C, sre, sim);
+}
+
+// Row pass for W <= 1024: one group of T lanes per row, warp FFT, no block
+// synchronisation.  Rows beyond H (only for tiny planes) compute on row H-1
+// and store nothing.
+constexpr int kRowWarps = 4;
+
+template <int W, int MODE>
+__global__ void __launch_bounds__(kRowWarps * 32, 4) row_pass_w(const RowArgs a)
+{
+    using WF = WarpFft<W>;
+    constexpr int T = WF::T, E = WF::E, G = 32 / T;
+    extern __shared__ float smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane / T, t = lane % T;
+    float *bre = smem + (warp * G + g) * WF::group_floats;
+    float *bim = bre + W;
+    const int H = a.d.H;
+    const int yr = blockIdx.x * (kRowWarps * G) + warp * G + g;
+    const bool valid = yr < H;
+    const int y = valid ? yr : H - 1;
+    const int p = blockIdx.y;
+    float2 *row = a.b.C + ((size_t)p * H + y) * W;
+    float2 v[E];
+
+    if (MODE == ROW_INIT) {
+#pragma unroll
+        for (int m = 0; m < E; m++)
+            v[m] = make_float2(0.f, 0.f);
+    } else {
+#pragma unroll
+        for (int m = 0; m < E; m++)
+            v[m] = row[t + T * m];
+        WF::template run<+1>(v, a.tw, bre, bim, t);
+    }
+    if (valid) {
+        const RowWork<MODE> work(a, p, y);
+#pragma unroll
+        for (int m = 0; m < E; m++)
+            work.apply(t + T * m, v[m]);
+    }
+    if (MODE == ROW_UPDATE && a.last)
+        return;
+    WF::template run<-1>(v, a.tw, bre, bim, t);
+    if (valid) {
+#pragma unroll
+        for (int m = 0; m < E; m++)
+            row[t + T * m] = v[m];
+    }
 }
 
 // --------------------------------------------------------- column pass
@@ -290,6 +361,85 @@ __global__ void split_estimate_kernel(const float2 *__restrict__ est, int nplane
         const size_t z = i / plane, r = i % plane;
         const float2 e = est[(z >> 1) * plane + r];
         out[i] = (z & 1) ? e.y : e.x;
+    }
+}
+
+// Column pass for H <= 1024: CW warps per block, G = 32 / T columns per
+// warp, FC = CW * G columns per block.  The FC-column tile is loaded into
+// shared memory with coalesced accesses (row stride FC + 1 floats keeps the
+// per-column reads free of bank conflicts), each group transforms its column
+// in registers using its own column of the tile as transpose buffer, and the
+// tile is written back.  Spectrum in launch layout: block bx, register m,
+// thread tid at spec[(bx * E + m) * (CW * 32) + tid].
+template <int H, int CW>
+__global__ void __launch_bounds__(CW * 32, 256 / CW) col_pass_w(const ColArgs a)
+{
+    using WF = WarpFft<H>;
+    constexpr int T = WF::T, E = WF::E, G = 32 / T, FC = CW * G, LD = FC + 1, NT = CW * 32;
+    extern __shared__ float smem[];
+    float *tre = smem;
+    float *tim = smem + H * LD;
+    const int W = a.W;
+    const int p = blockIdx.y;
+    const int x0 = blockIdx.x * FC;
+    float2 *C = a.C + (size_t)p * H * W + x0;
+
+    constexpr int units = H * FC / 2;
+#pragma unroll 4
+    for (int u = threadIdx.x; u < units; u += NT) {
+        const int c2 = u % (FC / 2), y = u / (FC / 2);
+        const float4 q = *reinterpret_cast<const float4 *>(C + (size_t)y * W + 2 * c2);
+        tre[y * LD + 2 * c2] = q.x;
+        tim[y * LD + 2 * c2] = q.y;
+        tre[y * LD + 2 * c2 + 1] = q.z;
+        tim[y * LD + 2 * c2 + 1] = q.w;
+    }
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane / T, t = lane % T;
+    const int c = warp * G + g;
+    float *cre = tre + c, *cim = tim + c;
+    float2 v[E];
+#pragma unroll
+    for (int m = 0; m < E; m++)
+        v[m] = make_float2(cre[(t + T * m) * LD], cim[(t + T * m) * LD]);
+    WF::template run<-1, LD>(v, a.tw, cre, cim, t);
+    const float2 *sp = a.spec + (size_t)blockIdx.x * E * NT + threadIdx.x;
+#pragma unroll
+    for (int m = 0; m < E; m++)
+        v[m] = cmul(v[m], __ldg(sp + (size_t)m * NT));
+    WF::template run<+1, LD>(v, a.tw, cre, cim, t);
+#pragma unroll
+    for (int m = 0; m < E; m++) {
+        cre[(t + T * m) * LD] = v[m].x;
+        cim[(t + T * m) * LD] = v[m].y;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int u = threadIdx.x; u < units; u += NT) {
+        const int c2 = u % (FC / 2), y = u / (FC / 2);
+        *reinterpret_cast<float4 *>(C + (size_t)y * W + 2 * c2) =
+            make_float4(tre[y * LD + 2 * c2], tim[y * LD + 2 * c2], tre[y * LD + 2 * c2 + 1], tim[y * LD + 2 * c2 + 1]);
+    }
+}
+
+// Launch layout of the column-pass spectrum for the warp engine.
+__global__ void permute_spectrum_w(const double2 *__restrict__ nat, float2 *__restrict__ out, int H, int W, int T,
+                                   int CW, double scale)
+{
+    const int E = H / T, G = 32 / T, FC = CW * G, NT = CW * 32;
+    const size_t total = (size_t)H * W;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int tid = (int)(i % NT);
+        const int m = (int)((i / NT) % E);
+        const int bx = (int)(i / ((size_t)NT * E));
+        const int warp = tid >> 5, lane = tid & 31;
+        const int g = lane / T, t = lane % T;
+        const int n = t + T * m;
+        const int col = bx * FC + warp * G + g;
+        const double2 k = nat[(size_t)n * W + col];
+        out[i] = make_float2((float)(k.x * scale), (float)(k.y * scale));
     }
 }
 
@@ -430,11 +580,23 @@ int snap_transform_size(int n)
 }
 
 static int sched_edge(int n) { return make_schedule(n).r[0]; }
-static int col_f_for(int H, int W);
+
+// Warps per column block of the warp engine: the largest of 8, 4, 2 whose
+// columns per block divide W.
+static int col_warps(int H, int W)
+{
+    const int G = 32 / warp_fft_lanes(H);
+    for (int cw = 8; cw > 1; cw /= 2)
+        if (W % (cw * G) == 0)
+            return cw;
+    return 1;
+}
 
 size_t rl_spectrum_elems(int H, int W)
 {
-    const int F = col_f_for(H, W);
+    if (H <= 1024)
+        return (size_t)H * W;
+    const int F = col_f(H);
     const int NT = F * H / kE;
     return (size_t)(W / F) * kE * NT;
 }
@@ -463,58 +625,62 @@ static void configure_smem(K kern, size_t bytes, unsigned &mask)
     }
 }
 
-// Rows per block: row_f(W) when it divides H, else 2 (tiny planes only).
-template <int W, int F, int MODE>
-static void launch_row_f(const RowArgs &a, cudaStream_t s)
-{
-    using C = Cfg<W, F>;
-    auto kern = row_pass<W, F, MODE>;
-    static unsigned mask = 0;
-    configure_smem(kern, C::smem, mask);
-    dim3 grid(a.d.H / F, a.b.npairs);
-    kern<<<grid, C::NT, C::smem, s>>>(a);
-    g_launches++;
-}
-
 template <int W, int MODE>
 static void launch_row(const RowArgs &a, cudaStream_t s)
 {
-    constexpr int F = row_f(W);
-    if constexpr (F > 2) {
-        if (a.d.H % F != 0) {
-            launch_row_f<W, 2, MODE>(a, s);
-            return;
-        }
+    if constexpr (W <= 1024) {
+        using WF = WarpFft<W>;
+        constexpr int G = 32 / WF::T;
+        constexpr size_t smem = sizeof(float) * kRowWarps * G * WF::group_floats;
+        auto kern = row_pass_w<W, MODE>;
+        static unsigned mask = 0;
+        configure_smem(kern, smem, mask);
+        dim3 grid((a.d.H + kRowWarps * G - 1) / (kRowWarps * G), a.b.npairs);
+        kern<<<grid, kRowWarps * 32, smem, s>>>(a);
+    } else {
+        constexpr int F = row_f(W);
+        using C = Cfg<W, F>;
+        auto kern = row_pass<W, F, MODE>;
+        static unsigned mask = 0;
+        configure_smem(kern, C::smem, mask);
+        dim3 grid(a.d.H / F, a.b.npairs);
+        kern<<<grid, C::NT, C::smem, s>>>(a);
     }
-    launch_row_f<W, F, MODE>(a, s);
-}
-
-template <int H, int F>
-static void launch_col_f(const ColArgs &a, int npairs, cudaStream_t s)
-{
-    using C = Cfg<H, F>;
-    auto kern = col_pass<H, F>;
-    static unsigned mask = 0;
-    configure_smem(kern, C::smem, mask);
-    dim3 grid(a.W / F, npairs);
-    kern<<<grid, C::NT, C::smem, s>>>(a);
     g_launches++;
 }
 
-// Columns per block: col_f(H) when it divides W, else 8 (tiny planes only).
-static int col_f_for(int H, int W) { return (W % col_f(H) == 0) ? col_f(H) : 8; }
+template <int H, int CW>
+static void launch_col_w(const ColArgs &a, int npairs, cudaStream_t s)
+{
+    using WF = WarpFft<H>;
+    constexpr int FC = CW * (32 / WF::T);
+    constexpr size_t smem = sizeof(float) * 2 * H * (FC + 1);
+    auto kern = col_pass_w<H, CW>;
+    static unsigned mask = 0;
+    configure_smem(kern, smem, mask);
+    dim3 grid(a.W / FC, npairs);
+    kern<<<grid, CW * 32, smem, s>>>(a);
+}
 
 template <int H>
 static void launch_col(const ColArgs &a, int npairs, cudaStream_t s)
 {
-    constexpr int F = col_f(H);
-    if constexpr (F > 8) {
-        if (a.W % F != 0) {
-            launch_col_f<H, 8>(a, npairs, s);
-            return;
+    if constexpr (H <= 1024) {
+        switch (col_warps(H, a.W)) {
+        case 8: launch_col_w<H, 8>(a, npairs, s); break;
+        case 4: launch_col_w<H, 4>(a, npairs, s); break;
+        default: launch_col_w<H, 2>(a, npairs, s); break;
         }
+    } else {
+        constexpr int F = col_f(H);
+        using C = Cfg<H, F>;
+        auto kern = col_pass<H, F>;
+        static unsigned mask = 0;
+        configure_smem(kern, C::smem, mask);
+        dim3 grid(a.W / F, npairs);
+        kern<<<grid, C::NT, C::smem, s>>>(a);
     }
-    launch_col_f<H, F>(a, npairs, s);
+    g_launches++;
 }
 
 template <int MODE>
@@ -529,27 +695,29 @@ static void dispatch_row(const RowArgs &a, cudaStream_t s)
     }
 }
 
+static const float2 *row_table(const RlDims &d, const RlTables &t) { return d.W <= 1024 ? t.wtwW : t.twW; }
+
 void rl_init(const RlDims &d, const RlBatch &b, const RlTables &t, cudaStream_t s)
 {
-    RowArgs a{d, b, t.twW, 0, 0};
+    RowArgs a{d, b, row_table(d, t), 0, 0};
     dispatch_row<ROW_INIT>(a, s);
 }
 
 void rl_divide(const RlDims &d, const RlBatch &b, const RlTables &t, int view, cudaStream_t s)
 {
-    RowArgs a{d, b, t.twW, view, 0};
+    RowArgs a{d, b, row_table(d, t), view, 0};
     dispatch_row<ROW_DIVIDE>(a, s);
 }
 
 void rl_update(const RlDims &d, const RlBatch &b, const RlTables &t, int view, bool last, cudaStream_t s)
 {
-    RowArgs a{d, b, t.twW, view, last ? 1 : 0};
+    RowArgs a{d, b, row_table(d, t), view, last ? 1 : 0};
     dispatch_row<ROW_UPDATE>(a, s);
 }
 
 void rl_col(const RlDims &d, const RlBatch &b, const RlTables &t, const float2 *spectrum, cudaStream_t s)
 {
-    ColArgs a{b.C, spectrum, t.twH, d.H, d.W};
+    ColArgs a{b.C, spectrum, d.H <= 1024 ? t.wtwH : t.twH, d.H, d.W};
     switch (d.H) {
 #define X(N) \
     case N: launch_col<N>(a, b.npairs, s); break;
@@ -559,6 +727,8 @@ void rl_col(const RlDims &d, const RlBatch &b, const RlTables &t, const float2 *
     }
 }
 
+int rl_warp_lanes(int n) { return n <= 1024 ? warp_fft_lanes(n) : 0; }
+
 void rl_kernel_spectrum(const float *d_kernel, int kH, int kW, int H, int W, const double2 *twH, const double2 *twW,
                         double2 *work, float2 *d_out, cudaStream_t s)
 {
@@ -566,12 +736,15 @@ void rl_kernel_spectrum(const float *d_kernel, int kH, int kW, int H, int W, con
     double2 *K = work + (size_t)kH * W;
     kspec_rows<<<dim3((W + 127) / 128, kH), 128, 0, s>>>(d_kernel, kH, kW, W, twW, A);
     kspec_cols<<<dim3((W + 127) / 128, H), 128, 0, s>>>(A, kH, H, W, twH, K);
-    const int F = col_f_for(H, W);
-    const int NT = F * H / kE;
-    const int R = sched_edge(H);
     const size_t total = rl_spectrum_elems(H, W);
-    permute_spectrum<<<(int)((total + 255) / 256 > 4096 ? 4096 : (total + 255) / 256), 256, 0, s>>>(
-        K, d_out, H, W, F, NT, R, 1.0 / ((double)H * (double)W));
+    const int blocks = (int)((total + 255) / 256 > 4096 ? 4096 : (total + 255) / 256);
+    const double scale = 1.0 / ((double)H * (double)W);
+    if (H <= 1024) {
+        permute_spectrum_w<<<blocks, 256, 0, s>>>(K, d_out, H, W, warp_fft_lanes(H), col_warps(H, W), scale);
+    } else {
+        const int F = col_f(H);
+        permute_spectrum<<<blocks, 256, 0, s>>>(K, d_out, H, W, F, F * H / kE, sched_edge(H), scale);
+    }
 }
 
 void rl_write_estimate(const RlDims &d, const RlBatch &b, cudaStream_t s)

@@ -36,9 +36,14 @@ struct RlBatch {
 
 // Per-plan constants that the kernels read.
 struct RlTables {
-    const float2 *twH;   // exp(-2 pi i n / H)
+    const float2 *twH;   // exp(-2 pi i n / H)            (lengths above 1024)
     const float2 *twW;   // exp(-2 pi i n / W)
+    const float2 *wtwH;  // warp-FFT twiddles of H: [k1 * T + t] = exp(-2 pi i t k1 / H)   (lengths <= 1024)
+    const float2 *wtwW;  // warp-FFT twiddles of W
 };
+
+// Lanes per line of the warp FFT for length n (0 when n > 1024).
+int rl_warp_lanes(int n);
 
 bool rl_length_supported(int n);
 // Number of kernel launches this library has issued (all kernels).

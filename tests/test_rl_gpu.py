@@ -180,3 +180,31 @@ def test_unsupported_size_reports_error():
     from gpu_deconvolution_b200.native import FmvdError
     with pytest.raises(FmvdError):
         api.DevicePlan(5000, 64, [np.ones((5000, 64), np.float32)], [np.ones((3, 3), np.float32)], 0)
+
+
+def test_cli_matches_c_api(tmp_path):
+    """The fmvd_deconvolve tool takes the reference CLI's flags
+    (fmvd_deconvolve_hdd.cpp:22-180) and writes the same planes."""
+    import os
+    import subprocess
+    from conftest import ROOT
+    exe = os.path.join(ROOT, "gpu_deconvolution_b200", "bin", "fmvd_deconvolve")
+    views, psfs, weights, _ = synth.plain_rl_views(shape=(4, 30, 34), n_views=2, n_beads=6, ksize=7, seed=15)
+    args = [exe, "-v", "2", "-i", "2", "-t", "0", "-o", str(tmp_path / "out.raw"), "-d"]
+    for v in range(2):
+        views[v].tofile(tmp_path / f"v{v}.raw")
+        args.append(str(tmp_path / f"v{v}.raw"))
+    args.append("-w")
+    for v in range(2):
+        weights[v].tofile(tmp_path / f"w{v}.raw")
+        args.append(str(tmp_path / f"w{v}.raw"))
+    args.append("-k")
+    for v in range(2):
+        psfs[v].tofile(tmp_path / f"k{v}.raw")
+        args.append(str(tmp_path / f"k{v}.raw"))
+    args += ["-dw", "34", "-dh", "30", "-dd", "4", "-kw", "7", "-kh", "7"]
+    r = subprocess.run(args, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    got = np.fromfile(tmp_path / "out.raw", np.uint16).reshape(-1, 30, 34)
+    want = api.deconvolve(views, weights, [p.copy() for p in psfs], 0, 2, nstreams=3)
+    assert np.array_equal(got, want)

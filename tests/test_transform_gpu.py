@@ -2,10 +2,11 @@
 hardware texture path of the reference resampler (texture-object
 restatement, oracle/_ref) and against the CPU oracle.
 
-Tolerance: the reference samples through the texture unit, whose weights
-have 1/256 granularity; the outputs here must agree within one sample unit
-(the rounding of v * 2^bits + 0.5 can flip on last-bit differences of v) and
-agree exactly in almost every voxel.
+Tolerance: against the CPU oracle (the same weight model) within one sample
+unit, the final rounding of v * 2^bits + 0.5.  Against the texture unit,
+whose 1/256 weight rounding differs from the model's by one step for some
+coordinates, within the change one weight step per axis can make (the
+oracle's transform_weight_sensitivity) plus one unit.
 """
 import os
 
@@ -55,7 +56,9 @@ def check_vs_texture_unit(got, ref, src, m, frame, bits):
     d = np.abs(got.astype(np.int64) - ref.astype(np.int64))
     d = np.minimum(d, bits_max + 1 - d)  # 0 and 2^bits - 1 are one wrap apart
     assert np.all(d <= sens + 1), (d - sens).max()
-    assert (d == 0).mean() > 0.5
+    if bits == 8:
+        # one 8-bit unit is 256 16-bit units: the weight rounding rarely shows
+        assert (d == 0).mean() > 0.5
 
 
 @pytest.mark.parametrize("bits", [16, 8])
