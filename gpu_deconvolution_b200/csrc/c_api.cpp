@@ -126,6 +126,13 @@ int fmvd_b200_deconvolve_device(fmvd_b200_plan *plan, const void *d_views, size_
                : 1;
 }
 
+int fmvd_b200_plan_check(fmvd_b200_plan *plan)
+{
+    if (!plan)
+        return 1;
+    return fmvd::engine_check_status(plan->eng) ? 0 : 1;
+}
+
 void fmvd_b200_plan_destroy(fmvd_b200_plan *plan)
 {
     if (!plan)

@@ -242,6 +242,7 @@ void deconvolve_planes(const typename Traits<S>::plan_t *plan, int iterations)
             break;
         }
     }
+    engine_check_status(e);
 }
 
 // fmvd_deconvolve_hdd.impl.cpp:16-76: the file source reads one plane per

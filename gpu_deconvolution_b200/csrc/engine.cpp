@@ -130,8 +130,10 @@ std::vector<double2> twiddles_d(int n)
     return t;
 }
 
-// Twiddles of the warp FFT's four-step split N = T x E: [k1 * T + t] =
-// exp(-2 pi i t k1 / N) for t < T, k1 < E (zeros when N has no warp split).
+// Twiddle table of the warp FFT's four-step split N = T x E (zeros when N
+// has no warp split): with R8 = min(E, 8) and J = E / R8,
+//   [j * T + t] = exp(-2 pi i R8 j t / N) for j < J, t < T
+//   [J * T + t] = exp(-2 pi i t / N)
 std::vector<float2> warp_twiddles(int n)
 {
     std::vector<float2> t(n, make_float2(0.f, 0.f));
@@ -139,11 +141,17 @@ std::vector<float2> warp_twiddles(int n)
     if (T == 0)
         return t;
     const int E = n / T;
-    for (int k1 = 0; k1 < E; k1++)
-        for (int l = 0; l < T; l++) {
-            const double a = -2.0 * M_PI * (double)((long long)l * k1 % n) / (double)n;
-            t[k1 * T + l] = make_float2((float)cos(a), (float)sin(a));
-        }
+    const int R8 = E < 8 ? E : 8;
+    const int J = E / R8;
+    auto w = [n](long long k) {
+        const double a = -2.0 * M_PI * (double)(k % n) / (double)n;
+        return make_float2((float)cos(a), (float)sin(a));
+    };
+    for (int j = 0; j < J; j++)
+        for (int l = 0; l < T; l++)
+            t[j * T + l] = w((long long)R8 * j * l);
+    for (int l = 0; l < T; l++)
+        t[J * T + l] = w(l);
     return t;
 }
 
@@ -226,7 +234,8 @@ Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weig
               FMVD_CHECK(cudaMalloc(&e->C, sizeof(float2) * (size_t)H * W * e->pairs_cap)) &&
               FMVD_CHECK(cudaMalloc(&e->est, sizeof(float2) * (size_t)H * W * e->pairs_cap)) &&
               FMVD_CHECK(cudaMalloc(&e->twH, sizeof(float2) * H)) && FMVD_CHECK(cudaMalloc(&e->twW, sizeof(float2) * W)) &&
-              FMVD_CHECK(cudaMalloc(&e->wtwH, sizeof(float2) * H)) && FMVD_CHECK(cudaMalloc(&e->wtwW, sizeof(float2) * W));
+              FMVD_CHECK(cudaMalloc(&e->wtwH, sizeof(float2) * H)) && FMVD_CHECK(cudaMalloc(&e->wtwW, sizeof(float2) * W)) &&
+              FMVD_CHECK(cudaMalloc(&e->status, sizeof(int))) && FMVD_CHECK(cudaMemset(e->status, 0, sizeof(int)));
     if (!ok) {
         engine_destroy(e);
         return nullptr;
@@ -303,6 +312,7 @@ void engine_destroy(Engine *e)
     cudaFree(e->twW);
     cudaFree(e->wtwH);
     cudaFree(e->wtwW);
+    cudaFree(e->status);
     delete e;
 }
 
@@ -321,6 +331,7 @@ void engine_batch(Engine *e, const void *data, size_t view_stride, void *out, in
     b.npairs = (nplanes + 1) / 2;
     b.nplanes = nplanes;
     b.init_value = 10.0f * (float)V;  // fmvd_deconvolve_cuda.impl.cu:62, once per view
+    b.status = e->status;
     RlTables t{e->twH, e->twW, e->wtwH, e->wtwW};
     const float2 *spec = e->spec;
     const size_t se = e->spec_elems;
@@ -341,6 +352,19 @@ void engine_batch(Engine *e, const void *data, size_t view_stride, void *out, in
                 rl_col(e->dims, b, t, spec + se * (2 * ((v + 1) % V)), s);
         }
     }
+}
+
+bool engine_check_status(Engine *e)
+{
+    int st = 0;
+    if (!FMVD_CHECK(cudaMemcpy(&st, e->status, sizeof(int), cudaMemcpyDeviceToHost)))
+        return false;
+    if (st) {
+        cudaMemset(e->status, 0, sizeof(int));
+        report_error("fmvd: a bulk copy into shared memory did not complete in time");
+        return false;
+    }
+    return true;
 }
 
 bool engine_run(Engine *e, const void *data, size_t view_stride, void *out, int nplanes, int iterations,

@@ -34,7 +34,8 @@ struct Engine {
     float2 *C;              // pairs_cap x H x W
     float2 *est;            // pairs_cap x H x W
     float2 *twH, *twW;      // exp(-2 pi i n / N), block engine
-    float2 *wtwH, *wtwW;    // warp engine: [k1 * T + t] = exp(-2 pi i t k1 / N)
+    float2 *wtwH, *wtwW;    // warp engine twiddle tables
+    int *status;            // device flag: a bulk-copy wait timed out
 };
 
 // Build an engine.  h_Kernel is normalised in place (reference semantics).
@@ -51,6 +52,10 @@ int default_pairs_cap(int H, int W);
 // planes of H x W.  Planes are processed in batches of 2 * pairs_cap.
 bool engine_run(Engine *e, const void *data, size_t view_stride, void *out, int nplanes, int iterations,
                 float *est_out, cudaStream_t s);
+
+// Reports (and clears) a timed-out bulk-copy wait flagged by the kernels;
+// false if one was flagged.  Synchronises with the device.
+bool engine_check_status(Engine *e);
 
 // Launch sequence of one batch (at most 2 * pairs_cap planes).
 void engine_batch(Engine *e, const void *data, size_t view_stride, void *out, int nplanes, int iterations,

@@ -25,6 +25,7 @@
 #include "fft_engine.cuh"
 #include "rl_kernels.h"
 #include "warp_fft.cuh"
+#include "tma_util.cuh"
 
 #include <math.h>
 #include <stdint.h>
@@ -68,6 +69,9 @@ struct RowArgs {
     const float2 *tw;
     int view;
     int last;
+    int bulk_data;      // data rows may be fetched with 16-byte bulk copies
+    int bulk_weights;   // weight rows may be fetched with 16-byte bulk copies
+    int group_floats;   // warp engine: shared floats per group (transpose + prefetch)
 };
 
 template <int W, int F>
@@ -107,10 +111,12 @@ __device__ __forceinline__ void store_rows(float2 *__restrict__ dst, const float
     }
 }
 
+// Sample loads and estimate traffic are streamed (evict-first in L2) so that
+// the batch's complex work planes stay resident in L2 between passes.
 __device__ __forceinline__ float load_sample(const void *base, size_t idx, int bits)
 {
-    return bits == 16 ? (float)__ldg(reinterpret_cast<const unsigned short *>(base) + idx)
-                      : (float)__ldg(reinterpret_cast<const unsigned char *>(base) + idx);
+    return bits == 16 ? (float)__ldcs(reinterpret_cast<const unsigned short *>(base) + idx)
+                      : (float)__ldcs(reinterpret_cast<const unsigned char *>(base) + idx);
 }
 
 // Float to sample as the reference's unpad kernel: clip at the maximum,
@@ -136,10 +142,13 @@ __device__ __forceinline__ void store_sample(void *base, size_t idx, float v, in
 template <int MODE>
 struct RowWork {
     const RlDims &d;
-    float2 *est;            // row y of the pair's estimate
+    float2 *est;             // row y of the pair's estimate (global)
+    const float2 *est_s;     // the same row prefetched into shared memory, or null
     const void *src0, *src1; // data rows (clamped) of planes 2p and 2p+1, view a.view
-    const float *wrow;      // weight row (clamped)
-    void *out0, *out1;      // output rows, or null
+    bool src_s;              // data rows are in shared memory
+    const float *wrow;       // weight row (clamped)
+    bool w_s;                // weight row is in shared memory
+    void *out0, *out1;       // output rows, or null
     bool has1;
     float init0, init1;
 
@@ -148,10 +157,12 @@ struct RowWork {
         const int W = d.W;
         has1 = 2 * p + 1 < a.b.nplanes;
         est = a.b.est + ((size_t)p * d.H + y) * W;
+        est_s = nullptr;
         init0 = a.b.init_value;
         init1 = has1 ? a.b.init_value : 0.f;
         const size_t es = d.bits == 16 ? 2 : 1;
         src0 = src1 = nullptr;
+        src_s = w_s = false;
         wrow = nullptr;
         out0 = out1 = nullptr;
         if (MODE == ROW_DIVIDE) {
@@ -169,26 +180,37 @@ struct RowWork {
         }
     }
 
+    __device__ __forceinline__ float sample(const void *row, int sx) const
+    {
+        if (src_s)
+            return d.bits == 16 ? (float)reinterpret_cast<const unsigned short *>(row)[sx]
+                                : (float)reinterpret_cast<const unsigned char *>(row)[sx];
+        return load_sample(row, sx, d.bits);
+    }
+
     __device__ __forceinline__ void apply(int x, float2 &v) const
     {
         if (MODE == ROW_INIT) {
             v = make_float2(init0, init1);
-            est[x] = v;
+            __stcs(est + x, v);
         } else if (MODE == ROW_DIVIDE) {
+            // q > 1 keeps the divisor in the range where the fast division is
+            // within 2 ulp of the IEEE quotient
             const int sx = clamp_src(x, d.dataW, d.bxD);
+            const float a0 = sample(src0, sx);
+            const float a1 = has1 ? sample(src1, sx) : 0.f;
             float2 q = v;
-            if (q.x > 1.f)
-                q.x = load_sample(src0, sx, d.bits) / q.x;
-            if (q.y > 1.f)
-                q.y = has1 ? load_sample(src1, sx, d.bits) / q.y : 0.f;
+            q.x = q.x > 1.f ? __fdividef(a0, q.x) : q.x;
+            q.y = q.y > 1.f ? __fdividef(a1, q.y) : q.y;
             v = q;
         } else {
-            const float w = __ldg(wrow + clamp_src(x, d.dataW, d.bxW));
-            float2 c = est[x];
+            const int sx = clamp_src(x, d.dataW, d.bxW);
+            const float w = w_s ? wrow[sx] : __ldg(wrow + sx);
+            float2 c = est_s ? est_s[x] : __ldcs(est + x);
             const float2 r = v;
             c.x += w * (c.x * r.x - c.x);
             c.y += w * (c.y * r.y - c.y);
-            est[x] = c;
+            __stcs(est + x, c);
             v = c;
             if (out0 && x < d.dataW) {
                 store_sample(out0, x, c.x, d.bits);
@@ -241,45 +263,131 @@ __global__ void __launch_bounds__(Cfg<W, F>::NT) row_pass(const RowArgs a)
 // Row pass for W <= 1024: one group of T lanes per row, warp FFT, no block
 // synchronisation.  Rows beyond H (only for tiny planes) compute on row H-1
 // and store nothing.
+// Occupancy knobs of the warp-engine passes (blocks per SM the register
+// allocation must allow, and the widest column block).
+#ifndef FMVD_ROW_MIN_BLOCKS
+#define FMVD_ROW_MIN_BLOCKS 4
+#endif
+#ifndef FMVD_COL_MIN_BLOCKS
+#define FMVD_COL_MIN_BLOCKS 2
+#endif
+#ifndef FMVD_COL_MAX_WARPS
+#define FMVD_COL_MAX_WARPS 8
+#endif
 constexpr int kRowWarps = 4;
 
 template <int W, int MODE>
-__global__ void __launch_bounds__(kRowWarps * 32, 4) row_pass_w(const RowArgs a)
+__global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_w(const RowArgs a)
 {
     using WF = WarpFft<W>;
     constexpr int T = WF::T, E = WF::E, G = 32 / T;
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) float smem[];
+    __shared__ __align__(8) uint64_t bars[kRowWarps * G];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane / T, t = lane % T;
-    float *bre = smem + (warp * G + g) * WF::group_floats;
+    const int gi = warp * G + g;
+    float *gbase = smem + (size_t)gi * a.group_floats;
+    float *bre = gbase;
     float *bim = bre + W;
+    char *pf = reinterpret_cast<char *>(gbase + WF::group_floats);  // prefetch area, 16-byte aligned
     const int H = a.d.H;
     const int yr = blockIdx.x * (kRowWarps * G) + warp * G + g;
     const bool valid = yr < H;
     const int y = valid ? yr : H - 1;
     const int p = blockIdx.y;
     float2 *row = a.b.C + ((size_t)p * H + y) * W;
-    float2 v[E];
+    RowWork<MODE> work(a, p, y);
 
+    // Rows the element-wise step needs are fetched by the bulk-copy engine
+    // while the inverse transform runs: the estimate and weight rows in the
+    // update pass, the two data rows in the divide pass.
+    const bool prefetch = MODE == ROW_UPDATE || (MODE == ROW_DIVIDE && a.bulk_data);
+    uint64_t *bar = &bars[gi];
+    if (prefetch) {
+        if (t == 0) {
+            mbar_init(bar, 1);
+            mbar_fence_init();
+        }
+        __syncwarp();
+        if (t == 0) {
+            const int es = a.d.bits == 16 ? 2 : 1;
+            if (MODE == ROW_UPDATE) {
+                const uint32_t eb = W * sizeof(float2);
+                const uint32_t wb = a.bulk_weights ? a.d.dataW * sizeof(float) : 0;
+                mbar_arrive_expect_tx(bar, eb + wb);
+                bulk_load(pf, work.est, eb, bar);
+                if (wb)
+                    bulk_load(pf + eb, work.wrow, wb, bar);
+            } else {
+                const uint32_t rb = a.d.dataW * es;
+                const uint32_t rs = (rb + 15) & ~15u;
+                mbar_arrive_expect_tx(bar, work.has1 ? 2 * rb : rb);
+                bulk_load(pf, work.src0, rb, bar);
+                if (work.has1)
+                    bulk_load(pf + rs, work.src1, rb, bar);
+            }
+        }
+    }
+
+    // One copy of the transform code serves both directions: the inverse is
+    // conj(DFT(conj(x))), so pass 0 (inverse of the loaded row) and pass 1
+    // (forward) run the same loop body; keeping it rolled halves the code the
+    // instruction cache must hold.
+    float2 v[E];
     if (MODE == ROW_INIT) {
 #pragma unroll
         for (int m = 0; m < E; m++)
             v[m] = make_float2(0.f, 0.f);
-    } else {
+        if (valid) {
+#pragma unroll
+            for (int m = 0; m < E; m++)
+                work.apply(t + T * m, v[m]);
+        }
+    }
+#pragma unroll 1
+    for (int pass = (MODE == ROW_INIT ? 1 : 0); pass < 2; pass++) {
+        if (pass == 0) {
+#pragma unroll
+            for (int m = 0; m < E; m++) {
+                const float2 x = row[t + T * m];
+                v[m] = make_float2(x.x, -x.y);
+            }
+        }
+        WF::template run<-1>(v, a.tw, bre, bim, t);
+        if (pass == 1)
+            break;
 #pragma unroll
         for (int m = 0; m < E; m++)
-            v[m] = row[t + T * m];
-        WF::template run<+1>(v, a.tw, bre, bim, t);
+            v[m].y = -v[m].y;
+    if (prefetch) {
+        if (!mbar_wait(bar, 0)) {
+            // the copy did not land in time: flag it, wait once more so no copy
+            // is left in flight, and continue from global memory
+            if (t == 0)
+                atomicExch(a.b.status, 1);
+            mbar_wait(bar, 0);
+        } else if (MODE == ROW_UPDATE) {
+            work.est_s = reinterpret_cast<const float2 *>(pf);
+            if (a.bulk_weights) {
+                work.wrow = reinterpret_cast<const float *>(pf + W * sizeof(float2));
+                work.w_s = true;
+            }
+        } else {
+            const int es = a.d.bits == 16 ? 2 : 1;
+            const uint32_t rs = (a.d.dataW * es + 15) & ~15u;
+            work.src0 = pf;
+            work.src1 = work.has1 ? pf + rs : pf;
+            work.src_s = true;
+        }
     }
     if (valid) {
-        const RowWork<MODE> work(a, p, y);
 #pragma unroll
         for (int m = 0; m < E; m++)
             work.apply(t + T * m, v[m]);
     }
     if (MODE == ROW_UPDATE && a.last)
         return;
-    WF::template run<-1>(v, a.tw, bre, bim, t);
+    }
     if (valid) {
 #pragma unroll
         for (int m = 0; m < E; m++)
@@ -364,21 +472,45 @@ __global__ void split_estimate_kernel(const float2 *__restrict__ est, int nplane
     }
 }
 
+// Column tile of the warp engine in shared memory: element (y, c) of the
+// block's FC columns.  With 32-lane groups the tile is dense and XOR-swizzled,
+// (y, c) at y * FC + (c ^ ((y >> SH) & (FC - 1))), SH = log2(32 / FC): the
+// coalesced row-wise fill, the per-column reads and the transposes of all
+// columns then each touch 32 distinct banks.  Smaller groups use a padded
+// row stride of FC + 1.
+template <int T, int FC>
+struct ColTile {
+    static constexpr bool swizzled = (T == 32) && FC > 1;
+    static constexpr int ld = swizzled ? FC : FC + 1;
+    static constexpr int sh = FC >= 32 ? 0 : (FC == 16 ? 1 : FC == 8 ? 2 : FC == 4 ? 3 : 4);
+    static __device__ __forceinline__ int at(int y, int c)
+    {
+        if constexpr (swizzled)
+            return y * FC + (c ^ ((y >> sh) & (FC - 1)));
+        else
+            return y * ld + c;
+    }
+    struct ColumnAddr {
+        int c;
+        __device__ __forceinline__ int operator()(int p) const { return at(p, c); }
+    };
+};
+
 // Column pass for H <= 1024: CW warps per block, G = 32 / T columns per
 // warp, FC = CW * G columns per block.  The FC-column tile is loaded into
-// shared memory with coalesced accesses (row stride FC + 1 floats keeps the
-// per-column reads free of bank conflicts), each group transforms its column
-// in registers using its own column of the tile as transpose buffer, and the
-// tile is written back.  Spectrum in launch layout: block bx, register m,
-// thread tid at spec[(bx * E + m) * (CW * 32) + tid].
+// shared memory with coalesced accesses, each group transforms its column in
+// registers using its own column of the tile as transpose buffer, and the tile
+// is written back.  Spectrum in launch layout: block bx, register m, thread
+// tid at spec[(bx * E + m) * (CW * 32) + tid].
 template <int H, int CW>
-__global__ void __launch_bounds__(CW * 32, 256 / CW) col_pass_w(const ColArgs a)
+__global__ void __launch_bounds__(CW * 32, FMVD_COL_MIN_BLOCKS) col_pass_w(const ColArgs a)
 {
     using WF = WarpFft<H>;
-    constexpr int T = WF::T, E = WF::E, G = 32 / T, FC = CW * G, LD = FC + 1, NT = CW * 32;
+    constexpr int T = WF::T, E = WF::E, G = 32 / T, FC = CW * G, NT = CW * 32;
+    using TL = ColTile<T, FC>;
     extern __shared__ float smem[];
     float *tre = smem;
-    float *tim = smem + H * LD;
+    float *tim = smem + H * TL::ld;
     const int W = a.W;
     const int p = blockIdx.y;
     const int x0 = blockIdx.x * FC;
@@ -389,38 +521,54 @@ __global__ void __launch_bounds__(CW * 32, 256 / CW) col_pass_w(const ColArgs a)
     for (int u = threadIdx.x; u < units; u += NT) {
         const int c2 = u % (FC / 2), y = u / (FC / 2);
         const float4 q = *reinterpret_cast<const float4 *>(C + (size_t)y * W + 2 * c2);
-        tre[y * LD + 2 * c2] = q.x;
-        tim[y * LD + 2 * c2] = q.y;
-        tre[y * LD + 2 * c2 + 1] = q.z;
-        tim[y * LD + 2 * c2 + 1] = q.w;
+        const int a0 = TL::at(y, 2 * c2), a1 = TL::at(y, 2 * c2 + 1);
+        tre[a0] = q.x;
+        tim[a0] = q.y;
+        tre[a1] = q.z;
+        tim[a1] = q.w;
     }
     __syncthreads();
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane / T, t = lane % T;
-    const int c = warp * G + g;
-    float *cre = tre + c, *cim = tim + c;
+    const typename TL::ColumnAddr addr{warp * G + g};
     float2 v[E];
 #pragma unroll
-    for (int m = 0; m < E; m++)
-        v[m] = make_float2(cre[(t + T * m) * LD], cim[(t + T * m) * LD]);
-    WF::template run<-1, LD>(v, a.tw, cre, cim, t);
+    for (int m = 0; m < E; m++) {
+        const int q = addr(t + T * m);
+        v[m] = make_float2(tre[q], tim[q]);
+    }
+    // pass 0: forward transform, times the spectrum, conjugated; pass 1: the
+    // same forward code gives the conjugate of the inverse transform
     const float2 *sp = a.spec + (size_t)blockIdx.x * E * NT + threadIdx.x;
+#pragma unroll 1
+    for (int pass = 0; pass < 2; pass++) {
+        WF::template run_addr<-1>(v, a.tw, tre, tim, t, addr);
+        if (pass == 1)
+            break;
 #pragma unroll
-    for (int m = 0; m < E; m++)
-        v[m] = cmul(v[m], __ldg(sp + (size_t)m * NT));
-    WF::template run<+1, LD>(v, a.tw, cre, cim, t);
+        for (int m0 = 0; m0 < E; m0 += 8) {
+            asm volatile("" ::: "memory");
+#pragma unroll
+            for (int m = m0; m < m0 + 8 && m < E; m++) {
+                const float2 z = cmul(v[m], __ldg(sp + (size_t)m * NT));
+                v[m] = make_float2(z.x, -z.y);
+            }
+        }
+        asm volatile("" ::: "memory");
+    }
 #pragma unroll
     for (int m = 0; m < E; m++) {
-        cre[(t + T * m) * LD] = v[m].x;
-        cim[(t + T * m) * LD] = v[m].y;
+        const int q = addr(t + T * m);
+        tre[q] = v[m].x;
+        tim[q] = -v[m].y;
     }
     __syncthreads();
 #pragma unroll 4
     for (int u = threadIdx.x; u < units; u += NT) {
         const int c2 = u % (FC / 2), y = u / (FC / 2);
-        *reinterpret_cast<float4 *>(C + (size_t)y * W + 2 * c2) =
-            make_float4(tre[y * LD + 2 * c2], tim[y * LD + 2 * c2], tre[y * LD + 2 * c2 + 1], tim[y * LD + 2 * c2 + 1]);
+        const int a0 = TL::at(y, 2 * c2), a1 = TL::at(y, 2 * c2 + 1);
+        *reinterpret_cast<float4 *>(C + (size_t)y * W + 2 * c2) = make_float4(tre[a0], tim[a0], tre[a1], tim[a1]);
     }
 }
 
@@ -586,7 +734,7 @@ static int sched_edge(int n) { return make_schedule(n).r[0]; }
 static int col_warps(int H, int W)
 {
     const int G = 32 / warp_fft_lanes(H);
-    for (int cw = 8; cw > 1; cw /= 2)
+    for (int cw = FMVD_COL_MAX_WARPS; cw > 1; cw /= 2)
         if (W % (cw * G) == 0)
             return cw;
     return 1;
@@ -625,16 +773,30 @@ static void configure_smem(K kern, size_t bytes, unsigned &mask)
     }
 }
 
+static bool aligned16(const void *p, size_t bytes) { return ((uintptr_t)p % 16 == 0) && bytes % 16 == 0; }
+
 template <int W, int MODE>
-static void launch_row(const RowArgs &a, cudaStream_t s)
+static void launch_row(const RowArgs &a0, cudaStream_t s)
 {
     if constexpr (W <= 1024) {
         using WF = WarpFft<W>;
         constexpr int G = 32 / WF::T;
-        constexpr size_t smem = sizeof(float) * kRowWarps * G * WF::group_floats;
+        RowArgs a = a0;
+        const size_t es = a.d.bits == 16 ? 2 : 1;
+        a.bulk_data = aligned16(a.b.data, a.d.dataW * es) && (a.b.view_stride * es) % 16 == 0 &&
+                      (a.b.plane_stride * es) % 16 == 0;
+        a.bulk_weights = aligned16(a.b.weights, a.d.dataW * sizeof(float)) &&
+                         ((size_t)a.d.dataH * a.d.dataW * sizeof(float)) % 16 == 0;
+        size_t pf = 0;
+        if (MODE == ROW_UPDATE)
+            pf = W * sizeof(float2) + (a.bulk_weights ? a.d.dataW * sizeof(float) : 0);
+        else if (MODE == ROW_DIVIDE && a.bulk_data)
+            pf = 2 * ((a.d.dataW * es + 15) & ~(size_t)15);
+        a.group_floats = WF::group_floats + (int)(pf / sizeof(float));
+        const size_t smem = sizeof(float) * kRowWarps * G * (size_t)a.group_floats;
         auto kern = row_pass_w<W, MODE>;
         static unsigned mask = 0;
-        configure_smem(kern, smem, mask);
+        configure_smem(kern, 200 * 1024, mask);
         dim3 grid((a.d.H + kRowWarps * G - 1) / (kRowWarps * G), a.b.npairs);
         kern<<<grid, kRowWarps * 32, smem, s>>>(a);
     } else {
@@ -643,8 +805,8 @@ static void launch_row(const RowArgs &a, cudaStream_t s)
         auto kern = row_pass<W, F, MODE>;
         static unsigned mask = 0;
         configure_smem(kern, C::smem, mask);
-        dim3 grid(a.d.H / F, a.b.npairs);
-        kern<<<grid, C::NT, C::smem, s>>>(a);
+        dim3 grid(a0.d.H / F, a0.b.npairs);
+        kern<<<grid, C::NT, C::smem, s>>>(a0);
     }
     g_launches++;
 }
@@ -654,7 +816,7 @@ static void launch_col_w(const ColArgs &a, int npairs, cudaStream_t s)
 {
     using WF = WarpFft<H>;
     constexpr int FC = CW * (32 / WF::T);
-    constexpr size_t smem = sizeof(float) * 2 * H * (FC + 1);
+    constexpr size_t smem = sizeof(float) * 2 * H * ColTile<WF::T, FC>::ld;
     auto kern = col_pass_w<H, CW>;
     static unsigned mask = 0;
     configure_smem(kern, smem, mask);
@@ -699,19 +861,19 @@ static const float2 *row_table(const RlDims &d, const RlTables &t) { return d.W 
 
 void rl_init(const RlDims &d, const RlBatch &b, const RlTables &t, cudaStream_t s)
 {
-    RowArgs a{d, b, row_table(d, t), 0, 0};
+    RowArgs a{d, b, row_table(d, t), 0, 0, 0, 0, 0};
     dispatch_row<ROW_INIT>(a, s);
 }
 
 void rl_divide(const RlDims &d, const RlBatch &b, const RlTables &t, int view, cudaStream_t s)
 {
-    RowArgs a{d, b, row_table(d, t), view, 0};
+    RowArgs a{d, b, row_table(d, t), view, 0, 0, 0, 0};
     dispatch_row<ROW_DIVIDE>(a, s);
 }
 
 void rl_update(const RlDims &d, const RlBatch &b, const RlTables &t, int view, bool last, cudaStream_t s)
 {
-    RowArgs a{d, b, row_table(d, t), view, last ? 1 : 0};
+    RowArgs a{d, b, row_table(d, t), view, last ? 1 : 0, 0, 0, 0};
     dispatch_row<ROW_UPDATE>(a, s);
 }
 

@@ -32,6 +32,7 @@ struct RlBatch {
     int npairs;
     int nplanes;
     float init_value;     // 10 * V
+    int *status;          // set to 1 by a kernel whose bulk copy wait timed out
 };
 
 // Per-plan constants that the kernels read.

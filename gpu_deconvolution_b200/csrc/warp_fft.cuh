@@ -131,21 +131,64 @@ struct WarpFft {
     // Position of transpose element (k1, t) inside a group's buffer.
     static __device__ __forceinline__ int tpos(int k1, int t) { return k1 * T + (t ^ (k1 & (T - 1))); }
 
+    // Twiddle table layout (per length N, built on the host, float2):
+    //   [j * T + t]       = w_N^(R8 j t)   for j < J   (R8 = min(E, 8), J = E / R8)
+    //   [J * T + t]       = w_N^t
+    // Lane t forms w_N^(t k1), k1 = R8 j + b, as table[j] * (w_N^t)^b with the
+    // powers b < R8 by repeated multiplication: J + 1 loads per transform
+    // instead of E - 1, and at most R8 rounding steps per twiddle.
+    static constexpr int R8 = E < 8 ? E : 8;
+    static constexpr int J = E / R8;
+    static constexpr int table_size = (J + 1) * T;
+
     // In-place transform of v (lane pattern v[m] = x[t + T m]).
-    // tw: w_N^(t k1) stored at [k1 * T + t] (forward table).  The transpose
-    // buffer element p lives at bre[p * STRIDE] / bim[p * STRIDE] (this
-    // group's shared memory); t: lane index inside the group.
+    // tw: twiddle table above.  The transpose buffer element p lives at
+    // bre[p * STRIDE] / bim[p * STRIDE] (this group's shared memory); t: lane
+    // index inside the group.
+    // Transpose buffer element p at bre[p * STRIDE] / bim[p * STRIDE].
+    template <int STRIDE>
+    struct StridedAddr {
+        __device__ __forceinline__ int operator()(int p) const { return p * STRIDE; }
+    };
+
     template <int DIR, int STRIDE = 1>
     static __device__ __forceinline__ void run(float2 *v, const float2 *__restrict__ tw, float *bre, float *bim,
                                                int t)
     {
+        run_addr<DIR>(v, tw, bre, bim, t, StridedAddr<STRIDE>());
+    }
+
+    // Same, with the transpose buffer element p at bre[addr(p)] / bim[addr(p)].
+    template <int DIR, typename Addr>
+    static __device__ __forceinline__ void run_addr(float2 *v, const float2 *__restrict__ tw, float *bre, float *bim,
+                                                    int t, const Addr &addr)
+    {
         Dft<E, DIR>::run(v);
+        {
+            const float2 w1 = __ldg(tw + J * T + t);
+            float2 wp[R8];
+            wp[0] = make_float2(1.f, 0.f);
+            if (R8 > 1)
+                wp[1] = w1;
 #pragma unroll
-        for (int k1 = 1; k1 < E; k1++)
-            v[k1] = ctw<DIR>(v[k1], __ldg(tw + k1 * T + t));
+            for (int b = 2; b < R8; b++)
+                wp[b] = cmul(wp[b - 1], w1);
+#pragma unroll
+            for (int j = 0; j < J; j++) {
+                const float2 wj = j == 0 ? make_float2(1.f, 0.f) : __ldg(tw + j * T + t);
+#pragma unroll
+                for (int b = 0; b < R8; b++) {
+                    const int k1 = j * R8 + b;
+                    if (k1 == 0)
+                        continue;
+                    const float2 w = j == 0 ? wp[b] : (b == 0 ? wj : cmul(wj, wp[b]));
+                    v[k1] = ctw<DIR>(v[k1], w);
+                }
+            }
+        }
 #pragma unroll
         for (int k1 = 0; k1 < E; k1++) {
-            const int p = tpos(k1, t) * STRIDE;
+            const int p = addr(tpos(k1, t));
             bre[p] = v[k1].x;
             bim[p] = v[k1].y;
         }
@@ -155,7 +198,7 @@ struct WarpFft {
             const int k1 = t + T * s;
 #pragma unroll
             for (int j = 0; j < T; j++) {
-                const int p = tpos(k1, j) * STRIDE;
+                const int p = addr(tpos(k1, j));
                 v[s * T + j] = make_float2(bre[p], bim[p]);
             }
         }

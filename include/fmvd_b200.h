@@ -29,6 +29,10 @@ int fmvd_b200_plan_query(const fmvd_b200_plan *plan, int *fftH, int *fftW, int *
  * receives nplanes float planes of fftH x fftW.  Asynchronous on stream. */
 int fmvd_b200_deconvolve_device(fmvd_b200_plan *plan, const void *d_views, size_t view_stride, void *d_out,
                                 int nplanes, int iterations, float *d_estimate, void *stream);
+/* Synchronises with the device and reports whether any kernel of the plan
+ * gave up waiting for a bulk copy (bounded waits never hang the GPU; a
+ * timeout is reported here as an error). */
+int fmvd_b200_plan_check(fmvd_b200_plan *plan);
 void fmvd_b200_plan_destroy(fmvd_b200_plan *plan);
 
 /* Streaming plans with an explicit batch size (the fmvd_initialize_cuda_*
