@@ -302,6 +302,14 @@ def run_b200(args):
     achieved = alg_bytes / t_rl / 1e9
     peak, peak_kind = peak_hbm()
     traffic = profiled_traffic()
+    # one unit of the roofline = one view update of one batch of plane pairs
+    # (the four passes row divide, column K^, row update, column K)
+    batch_planes = 2 * plan.pairs_per_batch
+    n_updates = -(-td // batch_planes) * V * ITERATIONS * args.steps
+    alg_per_update = BYTES_PER_PADDED_VOXEL_VIEW_ITER * H * W * batch_planes
+    traffic_per_update = None
+    if traffic and "bytes_per_view_update_per_padded_voxel" in traffic:
+        traffic_per_update = traffic["bytes_per_view_update_per_padded_voxel"] * H * W * batch_planes
 
     e2e = None
     if not args.no_e2e:
@@ -326,8 +334,12 @@ def run_b200(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "kernel": "fused RL view update (row divide, column K^, row update, column K passes)",
+                         "unit_of_work": f"one view update of a batch of {batch_planes} padded planes",
+                         "algorithmic_bytes_per_update": alg_per_update,
+                         "update_ms": t_rl / n_updates * 1e3,
                          "algorithmic_bytes": "14 B per padded voxel per view per iteration",
-                         "traffic": (traffic or {}).get("bytes_per_view_update_per_padded_voxel")},
+                         "traffic": traffic_per_update,
+                         "traffic_source": (traffic or {}).get("source")},
             "e2e": e2e,
             "cpu_baseline": cpu,
             "gpu_launches": int(launches),
