@@ -36,6 +36,7 @@ LIB_SOURCES = [
     "compat_launchers.cu",
     "transform.cu",
     "rl_kernels.cu",
+    "noalloc.cu",
 ]
 JNI_SOURCE = "jni/fastspim_NativeSPIMReconstructionCuda.cpp"
 

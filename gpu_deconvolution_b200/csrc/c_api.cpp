@@ -85,10 +85,6 @@ void transform_cuda_16(unsigned short **h_data, int w, int h, int d, int tw, int
 }
 
 // ---- fmvd_b200.h
-struct fmvd_b200_plan {
-    fmvd::Engine *eng;
-};
-
 fmvd_b200_plan *fmvd_b200_plan_create(int bits, int dataH, int dataW, const float *const *h_Weights, float **h_Kernel,
                                       int kernelH, int kernelW, fmvd_psf_type iteration_type, int nViews,
                                       int pairs_per_batch)

@@ -85,3 +85,8 @@ void transform_file(int bits, const void *const *h_planes, int w, int h, int d, 
                     const char *maskfile);
 
 } // namespace fmvd
+
+// Device-resident plan of the fmvd_b200_* entry points.
+struct fmvd_b200_plan {
+    fmvd::Engine *eng;
+};

@@ -90,6 +90,7 @@ SIGNATURES = {
     "fmvd_b200_deconvolve_device": (c_int, [c_p, c_p, C.c_size_t, c_p, c_int, c_int, c_p, c_p]),
     "fmvd_b200_plan_destroy": (None, [c_p]),
     "fmvd_b200_plan_check": (c_int, [c_p]),
+    "fmvd_b200_deconvolve_device_noalloc": (c_int, [c_p, c_p, C.c_size_t, c_p, c_int, c_int, c_p, c_p]),
     "fmvd_b200_initialize_cuda_16": (c_p, [c_int, c_int, c_p, c_p, c_int, c_int, c_int, c_int, c_int, SOURCE16,
                                            SINK16, c_int]),
     "fmvd_b200_initialize_cuda_8": (c_p, [c_int, c_int, c_p, c_p, c_int, c_int, c_int, c_int, c_int, SOURCE8, SINK8,
