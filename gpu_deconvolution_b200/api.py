@@ -169,7 +169,9 @@ def deconvolve_files(view_paths, out_path, dataW, dataH, dataD, weights, kernels
 class DevicePlan:
     """Device-resident deconvolution of torch CUDA tensors (fmvd_b200.h)."""
 
-    def __init__(self, dataH, dataW, weights, kernels, psf_type=0, bits=16, pairs_per_batch=0):
+    def __init__(self, dataH, dataW, weights, kernels, psf_type=0, bits=16, pairs_per_batch=0, col_warps=0):
+        """pairs_per_batch and col_warps are the two schedule knobs (0 =
+        automatic); ``autotune.tuned_plan`` picks them by measurement."""
         self.lib = native.load()
         self.bits = bits
         self.dataH, self.dataW = dataH, dataW
@@ -178,29 +180,83 @@ class DevicePlan:
         self.kernels = _kernel_arrays(kernels, self.V)
         kH, kW = self.kernels[0].shape
         native.clear_errors()
-        self.plan = self.lib.fmvd_b200_plan_create(bits, dataH, dataW, native.pointer_array(self.weights),
-                                                   native.pointer_array(self.kernels), kH, kW, int(psf_type), self.V,
-                                                   int(pairs_per_batch))
+        self.plan = None
+        if col_warps:
+            self.plan = self.lib.fmvd_b200_plan_create_tuned(bits, dataH, dataW, native.pointer_array(self.weights),
+                                                             native.pointer_array(self.kernels), kH, kW,
+                                                             int(psf_type), self.V, int(pairs_per_batch),
+                                                             int(col_warps))
+        else:
+            self.plan = self.lib.fmvd_b200_plan_create(bits, dataH, dataW, native.pointer_array(self.weights),
+                                                       native.pointer_array(self.kernels), kH, kW, int(psf_type),
+                                                       self.V, int(pairs_per_batch))
         native.check("fmvd_b200_plan_create")
         if not self.plan:
             raise FmvdError("plan creation failed")
         h, w, p = C.c_int(), C.c_int(), C.c_int()
         self.lib.fmvd_b200_plan_query(self.plan, C.byref(h), C.byref(w), C.byref(p))
         self.fftH, self.fftW, self.pairs_per_batch = h.value, w.value, p.value
+        self.col_warps = self.lib.fmvd_b200_plan_col_warps(self.plan)
 
-    def run(self, views, out, iterations, estimate=None, stream=0, view_stride=None, nplanes=None):
+    def run(self, views, out, iterations, estimate=None, stream=0, view_stride=None, nplanes=None, init=None):
         """views: CUDA tensor holding V x D x dataH x dataW samples;
         out: CUDA tensor with room for D x dataH x dataW samples; estimate:
-        optional float32 D x fftH x fftW.  ``nplanes`` defaults to out.shape[0].
-        Asynchronous on ``stream`` (an int handle)."""
+        optional float32 D x fftH x fftW that receives the final estimate;
+        init: optional float32 D x fftH x fftW to start from instead of the
+        reference's constant (continuing a run, or a warm start).
+        ``nplanes`` defaults to out.shape[0].  Asynchronous on ``stream``
+        (an int handle)."""
         D = nplanes if nplanes is not None else out.shape[0]
         vs = view_stride if view_stride is not None else D * self.dataH * self.dataW
+        est = estimate.data_ptr() if estimate is not None else None
         native.clear_errors()
-        r = self.lib.fmvd_b200_deconvolve_device(self.plan, views.data_ptr(), vs, out.data_ptr(), D, int(iterations),
-                                                 estimate.data_ptr() if estimate is not None else None, stream)
-        native.check("fmvd_b200_deconvolve_device")
+        if init is None:
+            name = "fmvd_b200_deconvolve_device"
+            r = self.lib.fmvd_b200_deconvolve_device(self.plan, views.data_ptr(), vs, out.data_ptr(), D,
+                                                     int(iterations), est, stream)
+        else:
+            name = "fmvd_b200_deconvolve_device_from"
+            r = self.lib.fmvd_b200_deconvolve_device_from(self.plan, views.data_ptr(), vs, out.data_ptr(), D,
+                                                          int(iterations), init.data_ptr(), est, stream)
+        native.check(name)
         if r != 0:
-            raise FmvdError("fmvd_b200_deconvolve_device failed")
+            raise FmvdError(name + " failed")
+
+    def pad_estimate(self, planes, out, stream=0):
+        """Data-plane float estimates (D x dataH x dataW CUDA tensor) onto the
+        FFT plane (``out``: D x fftH x fftW) with the views' border padding."""
+        native.clear_errors()
+        r = self.lib.fmvd_b200_pad_estimate(self.plan, planes.data_ptr(), out.data_ptr(), planes.shape[0], stream)
+        native.check("fmvd_b200_pad_estimate")
+        if r != 0:
+            raise FmvdError("fmvd_b200_pad_estimate failed")
+
+    def run_until(self, views, out, tol, max_iterations, check_every=5, init=None, stream=0):
+        """Plain RL in chunks of ``check_every`` iterations until the relative
+        change of every plane's estimate over one chunk,
+        ||e_k - e_(k-c)|| / ||e_k|| on the data region (FP64 sums on the
+        GPU), is at most ``tol``, or ``max_iterations`` ran.  Chunks continue
+        each other exactly.  Returns (iterations run, list of the largest
+        per-plane change after each chunk)."""
+        import torch
+        D = out.shape[0]
+        a = torch.empty((D, self.fftH, self.fftW), dtype=torch.float32, device=out.device)
+        b = torch.empty_like(a)
+        done, history = 0, []
+        cur = init
+        while done < max_iterations:
+            k = min(check_every, max_iterations - done)
+            self.run(views, out, k, estimate=a, stream=stream, init=cur)
+            done += k
+            if cur is not None:
+                st = plane_stats(a, cur, self.dataH, self.dataW, stream=stream)
+                change = float(np.max(np.sqrt(st[:, 2] / np.maximum(st[:, 1], 1e-300))))
+                history.append(change)
+                if change <= tol:
+                    break
+            a, b = b, a
+            cur = b
+        return done, history
 
     def destroy(self):
         if self.plan:
@@ -212,6 +268,68 @@ class DevicePlan:
             self.destroy()
         except Exception:
             pass
+
+
+class Batch:
+    """Several device-resident volumes (each with its own ``DevicePlan``)
+    deconvolved by one CUDA graph launch (fmvd_b200_batch_*).  The plans and
+    tensors must outlive the batch."""
+
+    def __init__(self, plans, views, outs, iterations, max_branches=8):
+        self.lib = native.load()
+        n = len(plans)
+        its = iterations if isinstance(iterations, (list, tuple)) else [iterations] * n
+        self._keep = (plans, views, outs)
+        P = (C.c_void_p * n)(*[p.plan for p in plans])
+        Vp = (C.c_void_p * n)(*[v.data_ptr() for v in views])
+        S = (C.c_size_t * n)(*[o.shape[0] * p.dataH * p.dataW for p, o in zip(plans, outs)])
+        O = (C.c_void_p * n)(*[o.data_ptr() for o in outs])
+        D = (C.c_int * n)(*[o.shape[0] for o in outs])
+        I = (C.c_int * n)(*[int(i) for i in its])
+        native.clear_errors()
+        self.batch = self.lib.fmvd_b200_batch_create(n, P, Vp, S, O, D, I, int(max_branches))
+        native.check("fmvd_b200_batch_create")
+        if not self.batch:
+            raise FmvdError("batch creation failed")
+        self.branches = self.lib.fmvd_b200_batch_branches(self.batch)
+
+    def run(self, stream=0):
+        native.clear_errors()
+        r = self.lib.fmvd_b200_batch_run(self.batch, stream)
+        native.check("fmvd_b200_batch_run")
+        if r != 0:
+            raise FmvdError("fmvd_b200_batch_run failed")
+
+    def destroy(self):
+        if self.batch:
+            self.lib.fmvd_b200_batch_destroy(self.batch)
+            self.batch = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def plane_stats(a, b=None, rows=None, cols=None, stream=0) -> np.ndarray:
+    """FP64 per-plane sums of CUDA float32 planes ``a`` (D x H x W) over the
+    top-left rows x cols region: columns sum a, sum a^2, sum (a-b)^2,
+    sum |a-b| (zero without ``b``).  Returns a D x 4 float64 array."""
+    import torch
+    D, H, W = a.shape
+    rows = H if rows is None else rows
+    cols = W if cols is None else cols
+    out = torch.empty((D, 4), dtype=torch.float64, device=a.device)
+    lib = native.load()
+    native.clear_errors()
+    r = lib.fmvd_b200_plane_stats(a.data_ptr(), b.data_ptr() if b is not None else None, D, H, W, rows, cols,
+                                  out.data_ptr(), stream)
+    native.check("fmvd_b200_plane_stats")
+    if r != 0:
+        raise FmvdError("fmvd_b200_plane_stats failed")
+    torch.cuda.synchronize(a.device)
+    return out.cpu().numpy()
 
 
 def transform_file(src: np.ndarray, inv, tw, th, td, outfile, mask=False, border=0, zspacing=1.0, maskfile=None):

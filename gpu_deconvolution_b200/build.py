@@ -37,6 +37,8 @@ LIB_SOURCES = [
     "transform.cu",
     "rl_kernels.cu",
     "noalloc.cu",
+    "stats.cu",
+    "batch.cpp",
 ]
 JNI_SOURCE = "jni/fastspim_NativeSPIMReconstructionCuda.cpp"
 

@@ -96,6 +96,19 @@ fmvd_b200_plan *fmvd_b200_plan_create(int bits, int dataH, int dataW, const floa
     return new fmvd_b200_plan{e};
 }
 
+fmvd_b200_plan *fmvd_b200_plan_create_tuned(int bits, int dataH, int dataW, const float *const *h_Weights,
+                                            float **h_Kernel, int kernelH, int kernelW, fmvd_psf_type iteration_type,
+                                            int nViews, int pairs_per_batch, int col_warps)
+{
+    fmvd::Engine *e = fmvd::engine_create(bits, dataH, dataW, h_Weights, h_Kernel, kernelH, kernelW, iteration_type,
+                                          nViews, pairs_per_batch, col_warps);
+    if (!e)
+        return nullptr;
+    return new fmvd_b200_plan{e};
+}
+
+int fmvd_b200_plan_col_warps(const fmvd_b200_plan *plan) { return plan ? plan->eng->dims.col_warps : -1; }
+
 int fmvd_b200_plan_query(const fmvd_b200_plan *plan, int *fftH, int *fftW, int *pairs)
 {
     if (!plan)
@@ -120,6 +133,40 @@ int fmvd_b200_deconvolve_device(fmvd_b200_plan *plan, const void *d_views, size_
                             (cudaStream_t)stream)
                ? 0
                : 1;
+}
+
+int fmvd_b200_deconvolve_device_from(fmvd_b200_plan *plan, const void *d_views, size_t view_stride, void *d_out,
+                                     int nplanes, int iterations, const float *d_init, float *d_estimate,
+                                     void *stream)
+{
+    if (!plan || nplanes < 0 || !d_init) {
+        fmvd::report_error("fmvd: invalid arguments to fmvd_b200_deconvolve_device_from");
+        return 1;
+    }
+    return fmvd::engine_run(plan->eng, d_views, view_stride, d_out, nplanes, iterations, d_estimate,
+                            (cudaStream_t)stream, d_init)
+               ? 0
+               : 1;
+}
+
+int fmvd_b200_pad_estimate(const fmvd_b200_plan *plan, const float *d_in, float *d_out, int nplanes, void *stream)
+{
+    if (!plan || nplanes < 0 || (nplanes > 0 && (!d_in || !d_out))) {
+        fmvd::report_error("fmvd: invalid arguments to fmvd_b200_pad_estimate");
+        return 1;
+    }
+    return fmvd::pad_estimate(d_in, d_out, nplanes, plan->eng->dims, (cudaStream_t)stream) ? 0 : 1;
+}
+
+int fmvd_b200_plane_stats(const float *d_a, const float *d_b, int nplanes, int H, int W, int rows, int cols,
+                          double *d_stats, void *stream)
+{
+    if (nplanes < 0 || H <= 0 || W <= 0 || rows < 0 || cols < 0 || rows > H || cols > W ||
+        (nplanes > 0 && (!d_a || !d_stats))) {
+        fmvd::report_error("fmvd: invalid arguments to fmvd_b200_plane_stats");
+        return 1;
+    }
+    return fmvd::plane_stats(d_a, d_b, nplanes, H, W, rows, cols, d_stats, (cudaStream_t)stream) ? 0 : 1;
 }
 
 int fmvd_b200_plan_check(fmvd_b200_plan *plan)

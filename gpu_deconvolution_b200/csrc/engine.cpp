@@ -173,7 +173,7 @@ int default_pairs_cap(int H, int W)
 }
 
 Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weights, float **h_Kernel, int kH,
-                      int kW, int psf_type, int nViews, int pairs_cap)
+                      int kW, int psf_type, int nViews, int pairs_cap, int col_warps)
 {
     if (bits != 8 && bits != 16) {
         report_error("fmvd: unsupported sample size");
@@ -188,6 +188,13 @@ Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weig
     if (!rl_length_supported(H) || !rl_length_supported(W)) {
         char msg[160];
         snprintf(msg, sizeof(msg), "fmvd: padded plane %d x %d is not supported (each side must be <= 4096)", H, W);
+        report_error(msg);
+        return nullptr;
+    }
+    const int cw = rl_col_warps(H, W, col_warps);
+    if (cw < 0) {
+        char msg[160];
+        snprintf(msg, sizeof(msg), "fmvd: %d column-pass warps do not fit a %d x %d plane", col_warps, H, W);
         report_error(msg);
         return nullptr;
     }
@@ -213,6 +220,7 @@ Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weig
     e->dims.bxD = kH / 2;
     e->dims.byW = kH / 2;
     e->dims.bxW = kW / 2;
+    e->dims.col_warps = cw;
     e->kH = kH;
     e->kW = kW;
     e->device = dev;
@@ -270,7 +278,7 @@ Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weig
                 ok = FMVD_CHECK(cudaMemcpy(d_k, src, sizeof(float) * kH * kW, cudaMemcpyHostToDevice));
                 if (ok) {
                     rl_kernel_spectrum(d_k, kH, kW, H, W, d_twH, d_twW, work,
-                                       e->spec + e->spec_elems * (2 * v + which), 0);
+                                       e->spec + e->spec_elems * (2 * v + which), e->dims.col_warps, 0);
                     ok = FMVD_CHECK(cudaGetLastError()) && FMVD_CHECK(cudaDeviceSynchronize());
                 }
             }
@@ -317,7 +325,7 @@ void engine_destroy(Engine *e)
 }
 
 void engine_batch(Engine *e, const void *data, size_t view_stride, void *out, int nplanes, int iterations,
-                  cudaStream_t s)
+                  cudaStream_t s, const float *init)
 {
     const int V = e->dims.V;
     RlBatch b;
@@ -331,6 +339,7 @@ void engine_batch(Engine *e, const void *data, size_t view_stride, void *out, in
     b.npairs = (nplanes + 1) / 2;
     b.nplanes = nplanes;
     b.init_value = 10.0f * (float)V;  // fmvd_deconvolve_cuda.impl.cu:62, once per view
+    b.init = init;
     b.status = e->status;
     RlTables t{e->twH, e->twW, e->wtwH, e->wtwW};
     const float2 *spec = e->spec;
@@ -368,7 +377,7 @@ bool engine_check_status(Engine *e)
 }
 
 bool engine_run(Engine *e, const void *data, size_t view_stride, void *out, int nplanes, int iterations,
-                float *est_out, cudaStream_t s)
+                float *est_out, cudaStream_t s, const float *init)
 {
     const size_t plane = (size_t)e->dims.dataH * e->dims.dataW;
     const size_t es = e->dims.bits == 16 ? 2 : 1;
@@ -376,7 +385,7 @@ bool engine_run(Engine *e, const void *data, size_t view_stride, void *out, int 
     for (int z0 = 0; z0 < nplanes; z0 += per) {
         const int n = nplanes - z0 < per ? nplanes - z0 : per;
         engine_batch(e, (const char *)data + z0 * plane * es, view_stride, (char *)out + z0 * plane * es, n,
-                     iterations, s);
+                     iterations, s, init ? init + (size_t)z0 * e->dims.H * e->dims.W : nullptr);
         if (est_out)
             rl_split_estimate(e->dims, e->est, n, est_out + (size_t)z0 * e->dims.H * e->dims.W, s);
         if (!FMVD_CHECK(cudaGetLastError()))

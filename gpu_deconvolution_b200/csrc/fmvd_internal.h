@@ -41,8 +41,9 @@ struct Engine {
 // Build an engine.  h_Kernel is normalised in place (reference semantics).
 // pairs_cap <= 0 selects the default batch size.  Returns null after
 // reporting an error.
+// col_warps: column-pass warps per block (2, 4 or 8; 0 = widest that fits).
 Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weights, float **h_Kernel, int kH,
-                      int kW, int psf_type, int nViews, int pairs_cap);
+                      int kW, int psf_type, int nViews, int pairs_cap, int col_warps = 0);
 void engine_destroy(Engine *e);
 int default_pairs_cap(int H, int W);
 
@@ -50,8 +51,11 @@ int default_pairs_cap(int H, int W);
 // input is at data + (v * view_stride + z * plane) samples; plane z of the
 // output at out + z * plane.  est_out (optional) receives nplanes float
 // planes of H x W.  Planes are processed in batches of 2 * pairs_cap.
+// init (optional): nplanes float planes of H x W to start from instead of the
+// reference's constant 10 * nViews; running k iterations from the estimate
+// that j iterations returned gives the result of j + k iterations.
 bool engine_run(Engine *e, const void *data, size_t view_stride, void *out, int nplanes, int iterations,
-                float *est_out, cudaStream_t s);
+                float *est_out, cudaStream_t s, const float *init = nullptr);
 
 // Reports (and clears) a timed-out bulk-copy wait flagged by the kernels;
 // false if one was flagged.  Synchronises with the device.
@@ -59,7 +63,7 @@ bool engine_check_status(Engine *e);
 
 // Launch sequence of one batch (at most 2 * pairs_cap planes).
 void engine_batch(Engine *e, const void *data, size_t view_stride, void *out, int nplanes, int iterations,
-                  cudaStream_t s);
+                  cudaStream_t s, const float *init = nullptr);
 
 // ---- plans and streaming (deconvolve.cpp)
 void *pinned_malloc(size_t size);
@@ -78,6 +82,11 @@ void deconvolve_files_8(FILE **f, FILE *r, int dW, int dH, int dD, float **w, fl
                         int V, int it);
 Engine *plan_engine_16(const fmvd_plan_cuda_16 *p);
 Engine *plan_engine_8(const fmvd_plan_cuda_8 *p);
+
+// ---- convergence statistics and warm-start padding (stats.cu)
+bool plane_stats(const float *a, const float *b, int nplanes, int H, int W, int rows, int cols, double *out,
+                 cudaStream_t s);
+bool pad_estimate(const float *in, float *out, int nplanes, const RlDims &d, cudaStream_t s);
 
 // ---- resampler (transform.cu)
 void transform_file(int bits, const void *const *h_planes, int w, int h, int d, int tw, int th, int td,

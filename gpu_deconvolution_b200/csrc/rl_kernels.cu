@@ -151,6 +151,7 @@ struct RowWork {
     void *out0, *out1;       // output rows, or null
     bool has1;
     float init0, init1;
+    const float *initr0, *initr1;  // rows of a given initial estimate, or null
 
     __device__ __forceinline__ RowWork(const RowArgs &a, int p, int y) : d(a.d)
     {
@@ -160,6 +161,11 @@ struct RowWork {
         est_s = nullptr;
         init0 = a.b.init_value;
         init1 = has1 ? a.b.init_value : 0.f;
+        initr0 = initr1 = nullptr;
+        if (MODE == ROW_INIT && a.b.init) {
+            initr0 = a.b.init + ((size_t)(2 * p) * d.H + y) * W;
+            initr1 = has1 ? a.b.init + ((size_t)(2 * p + 1) * d.H + y) * W : nullptr;
+        }
         const size_t es = d.bits == 16 ? 2 : 1;
         src0 = src1 = nullptr;
         src_s = w_s = false;
@@ -191,7 +197,8 @@ struct RowWork {
     __device__ __forceinline__ void apply(int x, float2 &v) const
     {
         if (MODE == ROW_INIT) {
-            v = make_float2(init0, init1);
+            v = initr0 ? make_float2(__ldcs(initr0 + x), initr1 ? __ldcs(initr1 + x) : 0.f)
+                       : make_float2(init0, init1);
             __stcs(est + x, v);
         } else if (MODE == ROW_DIVIDE) {
             // q > 1 keeps the divisor in the range where the fast division is
@@ -740,6 +747,18 @@ static int col_warps(int H, int W)
     return 1;
 }
 
+int rl_col_warps(int H, int W, int requested)
+{
+    if (H > 1024)
+        return 0;  // block engine: fixed column tile
+    if (requested == 0)
+        return col_warps(H, W);
+    const int G = 32 / warp_fft_lanes(H);
+    const bool ok = (requested == 2 || requested == 4 || requested == 8) && requested <= FMVD_COL_MAX_WARPS &&
+                    W % (requested * G) == 0;
+    return ok ? requested : -1;
+}
+
 size_t rl_spectrum_elems(int H, int W)
 {
     if (H <= 1024)
@@ -825,10 +844,10 @@ static void launch_col_w(const ColArgs &a, int npairs, cudaStream_t s)
 }
 
 template <int H>
-static void launch_col(const ColArgs &a, int npairs, cudaStream_t s)
+static void launch_col(const ColArgs &a, int npairs, int cw, cudaStream_t s)
 {
     if constexpr (H <= 1024) {
-        switch (col_warps(H, a.W)) {
+        switch (cw) {
         case 8: launch_col_w<H, 8>(a, npairs, s); break;
         case 4: launch_col_w<H, 4>(a, npairs, s); break;
         default: launch_col_w<H, 2>(a, npairs, s); break;
@@ -882,7 +901,7 @@ void rl_col(const RlDims &d, const RlBatch &b, const RlTables &t, const float2 *
     ColArgs a{b.C, spectrum, d.H <= 1024 ? t.wtwH : t.twH, d.H, d.W};
     switch (d.H) {
 #define X(N) \
-    case N: launch_col<N>(a, b.npairs, s); break;
+    case N: launch_col<N>(a, b.npairs, d.col_warps ? d.col_warps : col_warps(d.H, d.W), s); break;
         FMVD_FOR_EACH_LENGTH(X)
 #undef X
     default: break;
@@ -892,7 +911,7 @@ void rl_col(const RlDims &d, const RlBatch &b, const RlTables &t, const float2 *
 int rl_warp_lanes(int n) { return n <= 1024 ? warp_fft_lanes(n) : 0; }
 
 void rl_kernel_spectrum(const float *d_kernel, int kH, int kW, int H, int W, const double2 *twH, const double2 *twW,
-                        double2 *work, float2 *d_out, cudaStream_t s)
+                        double2 *work, float2 *d_out, int cw, cudaStream_t s)
 {
     double2 *A = work;
     double2 *K = work + (size_t)kH * W;
@@ -902,7 +921,8 @@ void rl_kernel_spectrum(const float *d_kernel, int kH, int kW, int H, int W, con
     const int blocks = (int)((total + 255) / 256 > 4096 ? 4096 : (total + 255) / 256);
     const double scale = 1.0 / ((double)H * (double)W);
     if (H <= 1024) {
-        permute_spectrum_w<<<blocks, 256, 0, s>>>(K, d_out, H, W, warp_fft_lanes(H), col_warps(H, W), scale);
+        permute_spectrum_w<<<blocks, 256, 0, s>>>(K, d_out, H, W, warp_fft_lanes(H), cw ? cw : col_warps(H, W),
+                                                  scale);
     } else {
         const int F = col_f(H);
         permute_spectrum<<<blocks, 256, 0, s>>>(K, d_out, H, W, F, F * H / kE, sched_edge(H), scale);

@@ -17,6 +17,7 @@ struct RlDims {
     int bits;            // 8 or 16 (sample type of data and output)
     int byD, bxD;
     int byW, bxW;
+    int col_warps;       // column-pass warps per block (warp engine, H <= 1024)
 };
 
 // One batch of plane pairs resident on the device.  Pair p packs planes
@@ -32,6 +33,7 @@ struct RlBatch {
     int npairs;
     int nplanes;
     float init_value;     // 10 * V
+    const float *init;    // optional initial estimate: nplanes x H x W floats (null: init_value everywhere)
     int *status;          // set to 1 by a kernel whose bulk copy wait timed out
 };
 
@@ -45,6 +47,9 @@ struct RlTables {
 
 // Lanes per line of the warp FFT for length n (0 when n > 1024).
 int rl_warp_lanes(int n);
+// Column-pass warps per block for an H x W plane: 'requested' (2, 4 or 8)
+// when the plane allows it, the widest allowed when 0, -1 when not allowed.
+int rl_col_warps(int H, int W, int requested);
 
 bool rl_length_supported(int n);
 // Number of kernel launches this library has issued (all kernels).
@@ -69,8 +74,9 @@ void rl_split_estimate(const RlDims &d, const float2 *est, int nplanes, float *o
 // Kernel spectrum of a kH x kW kernel centred at (kH/2, kW/2) -> (0, 0) on the
 // H x W plane, scaled by 1 / (H W), in the column-pass launch layout.
 // work must hold 2 * H * W + kH * W complex doubles.
+// col_warps: the plan's column-pass warps (the launch layout depends on it).
 void rl_kernel_spectrum(const float *d_kernel, int kH, int kW, int H, int W, const double2 *twH, const double2 *twW,
-                        double2 *work, float2 *d_out, cudaStream_t s);
+                        double2 *work, float2 *d_out, int col_warps, cudaStream_t s);
 // Weights normalised over views where the sum is positive.
 void rl_normalize_weights(const float *d_in, float *d_out, int V, size_t n, cudaStream_t s);
 // Clamp-to-border padded circular convolution of a dH x dW image with a

@@ -100,3 +100,74 @@ def rotation_y_inverse(angle_deg: float, frame_shape, src_shape, zscale: float, 
     M = S @ R
     t = S @ (cs - R @ c) + np.asarray(shift, np.float64) * np.array([1.0, 1.0, 1.0 / zscale])
     return np.concatenate([M, t[:, None]], axis=1).astype(np.float32).reshape(-1)
+
+
+# ----------------------------------------------------------------------------
+# Many uneven volumes (the batched workload): specifications on the host,
+# views generated on the GPU with torch (the same model as above: beads on a
+# background, per-plane blur, Poisson noise at a given peak).
+# ----------------------------------------------------------------------------
+BATCH_PLANE_SIZES = (128, 192, 256, 384, 512, 768, 1024)
+
+
+def batched_specs(seed: int = 0, count: int = 32, sizes=BATCH_PLANE_SIZES, depth=(16, 256), views=(2, 6),
+                  ksize=(9, 41), iterations: int = 25) -> list[dict]:
+    """Per-volume parameters: square planes from ``sizes``, depth U[depth],
+    views U[views], odd kernel size U[ksize], sigma_x U[0.8, 2], sigma_y
+    U[2, 6], a random in-plane angle per view, Poisson peak U[200, 5000]."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(count):
+        n = int(rng.choice(sizes))
+        k = int(rng.integers(ksize[0] // 2, ksize[1] // 2 + 1)) * 2 + 1
+        V = int(rng.integers(views[0], views[1] + 1))
+        specs.append({
+            "index": i, "H": n, "W": n, "D": int(rng.integers(depth[0], depth[1] + 1)), "V": V, "k": k,
+            "sigma": [[float(rng.uniform(0.8, 2.0)), float(rng.uniform(2.0, 6.0))] for _ in range(V)],
+            "angle": [float(rng.uniform(0.0, 180.0)) for _ in range(V)],
+            "peak": float(rng.uniform(200.0, 5000.0)), "iterations": iterations, "seed": int(rng.integers(1 << 30)),
+        })
+    return specs
+
+
+def spec_psfs(spec: dict) -> list[np.ndarray]:
+    k = spec["k"]
+    return [gaussian_psf(k, k, s[0], s[1], a) for s, a in zip(spec["sigma"], spec["angle"])]
+
+
+def views_torch(spec: dict, device="cuda", bits: int = 16, bead_density: float = 5e-5):
+    """V x D x H x W views of one volume on the GPU (torch int16 holding
+    uint16 bits for 16-bit samples, uint8 otherwise)."""
+    import torch
+    D, H, W, V = spec["D"], spec["H"], spec["W"], spec["V"]
+    g = torch.Generator(device=device).manual_seed(spec["seed"])
+    gt = torch.zeros((D, H, W), dtype=torch.float32, device=device)
+    n = max(1, int(bead_density * D * H * W))
+    idx = torch.randint(0, D * H * W, (n,), device=device, generator=g)
+    amp = torch.empty(n, device=device).uniform_(500.0, 2000.0, generator=g)
+    gt.view(-1).index_add_(0, idx, amp)
+    t = torch.arange(-3, 4, device=device, dtype=torch.float32)
+    b = torch.exp(-0.5 * t * t)
+    b = b / b.sum()
+    x = gt[None, None]
+    x = torch.nn.functional.conv3d(x, b.view(1, 1, 7, 1, 1), padding=(3, 0, 0))
+    x = torch.nn.functional.conv3d(x, b.view(1, 1, 1, 7, 1), padding=(0, 3, 0))
+    x = torch.nn.functional.conv3d(x, b.view(1, 1, 1, 1, 7), padding=(0, 0, 3))
+    gt = x[0, 0] * (1.0 / max(float(b.max()) ** 3, 1e-12)) + 100.0
+    gt = gt * (spec["peak"] / float(gt.max()))
+    out = torch.empty((V, D, H, W), dtype=torch.int16 if bits == 16 else torch.uint8, device=device)
+    mx = (1 << bits) - 1
+    for v, psf in enumerate(spec_psfs(spec)):
+        kH, kW = psf.shape
+        fh, fw = H + kH - 1, W + kW - 1
+        ks = torch.fft.rfft2(torch.from_numpy(psf).to(device), s=(fh, fw))
+        for z0 in range(0, D, 32):
+            z1 = min(z0 + 32, D)
+            full = torch.fft.irfft2(torch.fft.rfft2(gt[z0:z1], s=(fh, fw)) * ks, s=(fh, fw))
+            blurred = full[:, kH // 2:kH // 2 + H, kW // 2:kW // 2 + W].clamp_min(0)
+            noisy = torch.poisson(blurred, generator=g).clamp(0, mx).round()
+            if bits == 16:
+                out[v, z0:z1] = noisy.to(torch.int32).to(torch.int16)
+            else:
+                out[v, z0:z1] = noisy.to(torch.uint8)
+    return out

@@ -24,11 +24,39 @@ fmvd_b200_plan *fmvd_b200_plan_create(int bits, int dataH, int dataW, const floa
                                       float **h_Kernel, int kernelH, int kernelW, fmvd_psf_type iteration_type,
                                       int nViews, int pairs_per_batch);
 int fmvd_b200_plan_query(const fmvd_b200_plan *plan, int *fftH, int *fftW, int *pairs_per_batch);
+/* fmvd_b200_plan_create with the column-pass width as well: col_warps = 2, 4
+ * or 8 warps (columns) per block for padded planes up to 1024 rows, 0 for
+ * the widest the plane allows (the autotuner's two knobs are
+ * pairs_per_batch and col_warps). */
+fmvd_b200_plan *fmvd_b200_plan_create_tuned(int bits, int dataH, int dataW, const float *const *h_Weights,
+                                            float **h_Kernel, int kernelH, int kernelW, fmvd_psf_type iteration_type,
+                                            int nViews, int pairs_per_batch, int col_warps);
+/* Column-pass warps per block of the plan (0 for the block engine of planes
+ * above 1024 rows). */
+int fmvd_b200_plan_col_warps(const fmvd_b200_plan *plan);
 /* View v, plane z at d_views + (v * view_stride + z * dataH * dataW) samples;
  * output plane z at d_out + z * dataH * dataW.  d_estimate (optional)
  * receives nplanes float planes of fftH x fftW.  Asynchronous on stream. */
 int fmvd_b200_deconvolve_device(fmvd_b200_plan *plan, const void *d_views, size_t view_stride, void *d_out,
                                 int nplanes, int iterations, float *d_estimate, void *stream);
+/* fmvd_b200_deconvolve_device starting from d_init (nplanes float planes of
+ * fftH x fftW) instead of the constant 10 * nViews: iterations continue a
+ * previous run exactly when d_init is the estimate that run returned, and
+ * start from a warm-start estimate otherwise.  d_init may equal
+ * d_estimate. */
+int fmvd_b200_deconvolve_device_from(fmvd_b200_plan *plan, const void *d_views, size_t view_stride, void *d_out,
+                                     int nplanes, int iterations, const float *d_init, float *d_estimate,
+                                     void *stream);
+/* Estimates on the data plane (nplanes x dataH x dataW floats) onto the FFT
+ * plane (nplanes x fftH x fftW) with the clamp-to-border padding the views
+ * receive: the initial estimate of a warm start. */
+int fmvd_b200_pad_estimate(const fmvd_b200_plan *plan, const float *d_in, float *d_out, int nplanes, void *stream);
+/* Convergence check: per plane p of nplanes H x W float planes, in FP64 over
+ * rows < rows and columns < cols, d_stats[4p..4p+3] = sum a, sum a^2,
+ * sum (a - b)^2, sum |a - b| (d_b may be null: the last two are 0).
+ * Deterministic (fixed reduction order). */
+int fmvd_b200_plane_stats(const float *d_a, const float *d_b, int nplanes, int H, int W, int rows, int cols,
+                          double *d_stats, void *stream);
 /* Synchronises with the device and reports whether any kernel of the plan
  * gave up waiting for a bulk copy (bounded waits never hang the GPU; a
  * timeout is reported here as an error). */
@@ -47,6 +75,21 @@ void fmvd_b200_plan_destroy(fmvd_b200_plan *plan);
  * on one device race on the shared array: serialise them. */
 int fmvd_b200_deconvolve_device_noalloc(fmvd_b200_plan *plan, const void *d_views, size_t view_stride, void *d_out,
                                         int nplanes, int iterations, float *d_estimate, void *stream);
+
+/* ---- many volumes in one graph launch ------------------------------------ */
+/* Captures, once, the deconvolution of 'count' device-resident volumes
+ * (volume i: plans[i], d_views[i] with view_strides[i], d_outs[i],
+ * nplanes[i] planes, iterations[i]) into one CUDA graph with up to
+ * max_branches concurrent branches (0 = 8).  Volumes that share a plan run
+ * in order on one branch.  Buffers must stay valid while the batch exists. */
+typedef struct fmvd_b200_batch fmvd_b200_batch;
+fmvd_b200_batch *fmvd_b200_batch_create(int count, fmvd_b200_plan *const *plans, const void *const *d_views,
+                                        const size_t *view_strides, void *const *d_outs, const int *nplanes,
+                                        const int *iterations, int max_branches);
+/* One graph launch on stream: every volume of the batch, asynchronously. */
+int fmvd_b200_batch_run(fmvd_b200_batch *batch, void *stream);
+int fmvd_b200_batch_branches(const fmvd_b200_batch *batch);
+void fmvd_b200_batch_destroy(fmvd_b200_batch *batch);
 
 /* Streaming plans with an explicit batch size (the fmvd_initialize_cuda_*
  * entry points choose it automatically). */

@@ -343,6 +343,26 @@ def transformed_mask(inv: np.ndarray, z: int, w: int, h: int, d: int, zspacing: 
 # --------------------------------------------------------------------------
 # Plane streaming call pattern (fmvd_deconvolve.impl.cpp:205-300)
 # --------------------------------------------------------------------------
+def plane_stats(a: np.ndarray, b: np.ndarray | None = None, rows: int | None = None,
+                cols: int | None = None) -> np.ndarray:
+    """FP64 per-plane sums of the convergence check (no reference
+    counterpart): sum a, sum a^2, sum (a-b)^2, sum |a-b| over the top-left
+    rows x cols of each plane."""
+    a = np.asarray(a, np.float64)
+    D, H, W = a.shape
+    rows = H if rows is None else rows
+    cols = W if cols is None else cols
+    aa = a[:, :rows, :cols]
+    out = np.zeros((D, 4))
+    out[:, 0] = aa.sum(axis=(1, 2))
+    out[:, 1] = (aa * aa).sum(axis=(1, 2))
+    if b is not None:
+        d = aa - np.asarray(b, np.float64)[:, :rows, :cols]
+        out[:, 2] = (d * d).sum(axis=(1, 2))
+        out[:, 3] = np.abs(d).sum(axis=(1, 2))
+    return out
+
+
 def streaming_call_counts(n_planes: int, n_streams: int) -> tuple[int, int]:
     """Number of datasource and datasink calls the reference driver makes for
     a source holding ``n_planes`` planes: it primes ``n_streams`` slots without

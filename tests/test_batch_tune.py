@@ -1,0 +1,155 @@
+"""Many volumes in one graph launch (fmvd_b200_batch_*) and the schedule
+autotuner.  CPU tests cover the tuner's cache and choice; GPU tests check
+that a batched graph run and a tuned plan give exactly the per-volume
+results of the default path, and that a batched volume matches the oracle."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from gpu_deconvolution_b200 import autotune, synth
+
+
+def test_best_prefers_fastest_then_smaller():
+    table = {(2, 4): 1.0, (4, 8): 0.8, (6, 2): 0.8, (1, 2): 3.0}
+    assert autotune.best(table) == (4, 8)
+    assert autotune.best({(3, 8): 1.0, (3, 4): 1.0}) == (3, 4)
+
+
+def test_pair_candidates_bounded_by_memory():
+    assert autotune.pair_candidates(512, 512) == list(autotune.PAIRS)
+    big = autotune.pair_candidates(4096, 4096)
+    assert big and all(p * 2 * 8 * 4096 * 4096 <= autotune.MAX_WORK_BYTES for p in big) or big == [1]
+
+
+def test_cache_roundtrip(tmp_path):
+    path = str(tmp_path / "tune.json")
+    key = autotune.cache_key("B200", 1024, 1024, 4, 16)
+    assert autotune.load_cache(path) == {}
+    autotune.save_entry(key, {"pairs_per_batch": 6, "col_warps": 8}, path)
+    autotune.save_entry("other", {"pairs_per_batch": 1, "col_warps": 2}, path)
+    data = autotune.load_cache(path)
+    assert data[key]["pairs_per_batch"] == 6 and "other" in data
+    (tmp_path / "bad.json").write_text("not json")
+    assert autotune.load_cache(str(tmp_path / "bad.json")) == {}
+
+
+def test_batched_specs_follow_the_workload():
+    specs = synth.batched_specs(0, 32)
+    assert len(specs) == 32
+    for s in specs:
+        assert s["H"] == s["W"] and s["H"] in synth.BATCH_PLANE_SIZES
+        assert 16 <= s["D"] <= 256 and 2 <= s["V"] <= 6
+        assert s["k"] % 2 == 1 and 9 <= s["k"] <= 41
+        assert 200 <= s["peak"] <= 5000 and len(s["sigma"]) == s["V"]
+    assert synth.batched_specs(0, 32) == specs  # seeded
+
+
+def _small_specs():
+    return synth.batched_specs(5, 4, sizes=(64, 96, 128), depth=(3, 7), views=(2, 3), ksize=(5, 11),
+                               iterations=6)
+
+
+@pytest.mark.gpu
+def test_batch_graph_matches_individual_runs():
+    import torch
+    from gpu_deconvolution_b200 import api
+    specs = _small_specs()
+    plans, views, outs, refs = [], [], [], []
+    for s in specs:
+        psfs = synth.spec_psfs(s)
+        w = [np.ones((s["H"], s["W"]), np.float32)] * s["V"]
+        plans.append(api.DevicePlan(s["H"], s["W"], w, psfs, 0))
+        views.append(synth.views_torch(s))
+        outs.append(torch.zeros((s["D"], s["H"], s["W"]), dtype=torch.int16, device="cuda"))
+    # a fifth volume that shares the first plan (same branch, run in order)
+    views.append(views[0].flip(1).contiguous())
+    outs.append(torch.zeros_like(outs[0]))
+    all_plans = plans + [plans[0]]
+    its = [s["iterations"] for s in specs] + [specs[0]["iterations"]]
+    try:
+        for p, v, o, it in zip(all_plans, views, outs, its):
+            ref = torch.zeros_like(o)
+            p.run(v, ref, it)
+            refs.append(ref)
+        torch.cuda.synchronize()
+        batch = api.Batch(all_plans, views, outs, its, max_branches=3)
+        try:
+            assert batch.branches == 3
+            for _ in range(2):  # graph replay gives the same result
+                for o in outs:
+                    o.zero_()
+                batch.run()
+                torch.cuda.synchronize()
+                for o, r in zip(outs, refs):
+                    assert torch.equal(o, r)
+        finally:
+            batch.destroy()
+        for p in plans:
+            assert p.lib.fmvd_b200_plan_check(p.plan) == 0
+    finally:
+        for p in plans:
+            p.destroy()
+
+
+@pytest.mark.gpu
+def test_batched_volume_against_oracle():
+    """Per-volume error of a batched volume against the FP64 oracle on two
+    planes (RL parity tolerance 1e-4 relative L2 on the estimate)."""
+    import torch
+    from gpu_deconvolution_b200 import api
+    from oracle import fmvd_oracle as O
+    s = _small_specs()[1]
+    psfs = synth.spec_psfs(s)
+    w = [np.ones((s["H"], s["W"]), np.float32)] * s["V"]
+    plan = api.DevicePlan(s["H"], s["W"], w, [p.copy() for p in psfs], 0)
+    try:
+        views = synth.views_torch(s)
+        out = torch.zeros((s["D"], s["H"], s["W"]), dtype=torch.int16, device="cuda")
+        est = torch.zeros((s["D"], plan.fftH, plan.fftW), dtype=torch.float32, device="cuda")
+        plan.run(views, out, s["iterations"], estimate=est)
+        torch.cuda.synchronize()
+        vnp = views.cpu().numpy().view(np.uint16)
+        oplan = O.Plan(s["H"], s["W"], w, psfs, 0)
+        for z in (0, s["D"] - 1):
+            e = oplan.deconvolve_plane([vnp[v, z] for v in range(s["V"])], s["iterations"])
+            assert rel_l2(est[z].cpu().numpy(), e) < 1e-4
+    finally:
+        plan.destroy()
+
+
+@pytest.mark.gpu
+def test_tuned_plan_is_bit_identical(tmp_path):
+    import torch
+    from gpu_deconvolution_b200 import api
+    H, W, V, D, k = 120, 100, 3, 9, 9
+    entry = autotune.tune(H, W, k, k, views=V, planes=12, iterations=1, repeats=1,
+                          path=str(tmp_path / "t.json"))
+    assert entry["pairs_per_batch"] in autotune.PAIRS and entry["col_warps"] in (2, 4, 8)
+    assert autotune.load_cache(str(tmp_path / "t.json"))  # cached
+    psfs = [synth.gaussian_psf(k, k, 1.0, 2.0, 30.0 * v) for v in range(V)]
+    w = [np.ones((H, W), np.float32)] * V
+    g = torch.Generator(device="cuda").manual_seed(3)
+    views = torch.randint(50, 3000, (V, D, H, W), dtype=torch.int32, device="cuda", generator=g).to(torch.int16)
+    tuned = autotune.tuned_plan(H, W, w, [p.copy() for p in psfs], path=str(tmp_path / "t.json"))
+    default = api.DevicePlan(H, W, w, [p.copy() for p in psfs], 0)
+    try:
+        a = torch.zeros((D, H, W), dtype=torch.int16, device="cuda")
+        b = torch.zeros_like(a)
+        ea = torch.zeros((D, tuned.fftH, tuned.fftW), dtype=torch.float32, device="cuda")
+        eb = torch.zeros_like(ea)
+        tuned.run(views, a, 5, estimate=ea)
+        default.run(views, b, 5, estimate=eb)
+        torch.cuda.synchronize()
+        assert torch.equal(ea, eb) and torch.equal(a, b)
+        # every column width gives the same bits
+        for cw in (2, 4, 8):
+            p = api.DevicePlan(H, W, w, [q.copy() for q in psfs], 0, pairs_per_batch=2, col_warps=cw)
+            try:
+                p.run(views, a, 5, estimate=ea)
+                torch.cuda.synchronize()
+                assert p.col_warps == cw and torch.equal(ea, eb)
+            finally:
+                p.destroy()
+    finally:
+        tuned.destroy()
+        default.destroy()
