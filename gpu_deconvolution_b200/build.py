@@ -39,6 +39,8 @@ LIB_SOURCES = [
     "noalloc.cu",
     "stats.cu",
     "batch.cpp",
+    "unet_gemm.cu",
+    "unet_capi.cpp",
 ]
 JNI_SOURCE = "jni/fastspim_NativeSPIMReconstructionCuda.cpp"
 

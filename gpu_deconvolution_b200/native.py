@@ -91,6 +91,9 @@ SIGNATURES = {
     "fmvd_b200_plan_destroy": (None, [c_p]),
     "fmvd_b200_plan_check": (c_int, [c_p]),
     "fmvd_b200_deconvolve_device_noalloc": (c_int, [c_p, c_p, C.c_size_t, c_p, c_int, c_int, c_p, c_p]),
+    "fmvd_b200_conv_bf16": (c_int, [c_p, c_p, c_int, c_int, c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p, c_p,
+                                    c_int, c_p, c_p]),
+    "fmvd_b200_conv_wgrad_bf16": (c_int, [c_p, c_p, c_int, c_int, c_int, c_int, c_int, c_int, c_p, c_p, c_p]),
     "fmvd_b200_batch_create": (c_p, [c_int, c_p, c_p, c_p, c_p, c_p, c_p, c_int]),
     "fmvd_b200_batch_run": (c_int, [c_p, c_p]),
     "fmvd_b200_batch_branches": (c_int, [c_p]),

@@ -120,6 +120,22 @@ int fmvd_b200_mask_device(float *d_out, int z, int w, int h, int d, float zspaci
 int fmvd_b200_transform_host(int bits, const void *const *h_planes, int w, int h, int d, int tw, int th, int td,
                              const float *h_inverse, void *h_out);
 
+/* ---- tensor-core convolutions of the warm-start network ------------------ */
+/* BF16 NHWC activations, weights [cout][taps][cin] (taps 9 = 3 x 3 with zero
+ * padding, or 1), FP32 accumulation on the tcgen05 tensor cores:
+ * out = relu?(conv(in, weight) + bias + add), zeroed where mask <= 0;
+ * d_out (bf16) and/or d_out_f32 receive N x H x W x cout.  cin a multiple of
+ * 32, cout a multiple of 16 (at most 256, or a multiple of 256), W a multiple
+ * of 8 that divides 128 or is divided by it.  d_status (optional) is set to 1
+ * if a wait inside the kernel timed out. */
+int fmvd_b200_conv_bf16(const void *d_in, const void *d_weight, int N, int H, int W, int cin, int cout, int taps,
+                        void *d_out, float *d_out_f32, const float *d_bias, const void *d_add, const void *d_mask,
+                        int relu, int *d_status, void *stream);
+/* Weight gradient: d_dw[co][t][ci] += sum over pixels of
+ * grad[p][co] * in[p + offset(t)][ci] (FP32, accumulated atomically). */
+int fmvd_b200_conv_wgrad_bf16(const void *d_grad, const void *d_in, int N, int H, int W, int cin, int cout, int taps,
+                              float *d_dw, int *d_status, void *stream);
+
 /* ---- instrumentation ----------------------------------------------------- */
 /* Number of kernel launches the library has issued in this process. */
 unsigned long long fmvd_b200_launch_count(void);
