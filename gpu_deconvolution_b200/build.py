@@ -41,6 +41,8 @@ LIB_SOURCES = [
     "batch.cpp",
     "unet_gemm.cu",
     "unet_capi.cpp",
+    "unet_layers.cu",
+    "unet_model.cpp",
 ]
 JNI_SOURCE = "jni/fastspim_NativeSPIMReconstructionCuda.cpp"
 

@@ -94,6 +94,15 @@ SIGNATURES = {
     "fmvd_b200_conv_bf16": (c_int, [c_p, c_p, c_int, c_int, c_int, c_int, c_int, c_int, c_p, c_p, c_p, c_p, c_p,
                                     c_int, c_p, c_p]),
     "fmvd_b200_conv_wgrad_bf16": (c_int, [c_p, c_p, c_int, c_int, c_int, c_int, c_int, c_int, c_p, c_p, c_p]),
+    "fmvd_b200_unet_create": (c_p, [c_int, c_int, c_int, c_int, C.c_uint]),
+    "fmvd_b200_unet_destroy": (None, [c_p]),
+    "fmvd_b200_unet_param_count": (C.c_size_t, [c_p]),
+    "fmvd_b200_unet_get_params": (c_int, [c_p, c_p]),
+    "fmvd_b200_unet_set_params": (c_int, [c_p, c_p]),
+    "fmvd_b200_unet_get_grads": (c_int, [c_p, c_p]),
+    "fmvd_b200_unet_forward": (c_int, [c_p, c_p, C.c_size_t, c_int, c_p, c_p]),
+    "fmvd_b200_unet_train_step": (c_int, [c_p, c_p, C.c_size_t, c_int, c_p, C.c_float, c_p, c_p]),
+    "fmvd_b200_unet_check": (c_int, [c_p]),
     "fmvd_b200_batch_create": (c_p, [c_int, c_p, c_p, c_p, c_p, c_p, c_p, c_int]),
     "fmvd_b200_batch_run": (c_int, [c_p, c_p]),
     "fmvd_b200_batch_branches": (c_int, [c_p]),

@@ -135,39 +135,65 @@ def spec_psfs(spec: dict) -> list[np.ndarray]:
     return [gaussian_psf(k, k, s[0], s[1], a) for s, a in zip(spec["sigma"], spec["angle"])]
 
 
-def views_torch(spec: dict, device="cuda", bits: int = 16, bead_density: float = 5e-5):
-    """V x D x H x W views of one volume on the GPU (torch int16 holding
-    uint16 bits for 16-bit samples, uint8 otherwise)."""
+def bead_volume_torch(D, H, W, seed, device="cuda", density=5e-5, amp=(500.0, 2000.0), background=100.0,
+                      sigma=1.0):
+    """Ground truth on the GPU: Gaussian beads (width ``sigma`` voxels,
+    amplitude U[amp]) at ``density`` beads per voxel on ``background``."""
     import torch
-    D, H, W, V = spec["D"], spec["H"], spec["W"], spec["V"]
-    g = torch.Generator(device=device).manual_seed(spec["seed"])
+    g = torch.Generator(device=device).manual_seed(int(seed))
     gt = torch.zeros((D, H, W), dtype=torch.float32, device=device)
-    n = max(1, int(bead_density * D * H * W))
+    n = max(1, int(density * D * H * W))
     idx = torch.randint(0, D * H * W, (n,), device=device, generator=g)
-    amp = torch.empty(n, device=device).uniform_(500.0, 2000.0, generator=g)
-    gt.view(-1).index_add_(0, idx, amp)
-    t = torch.arange(-3, 4, device=device, dtype=torch.float32)
-    b = torch.exp(-0.5 * t * t)
-    b = b / b.sum()
+    a = torch.empty(n, device=device).uniform_(amp[0], amp[1], generator=g)
+    gt.view(-1).index_add_(0, idx, a)
+    r = int(np.ceil(3 * sigma))
+    t = torch.arange(-r, r + 1, device=device, dtype=torch.float32)
+    b = torch.exp(-0.5 * (t / sigma) ** 2)
+    k = 2 * r + 1
     x = gt[None, None]
-    x = torch.nn.functional.conv3d(x, b.view(1, 1, 7, 1, 1), padding=(3, 0, 0))
-    x = torch.nn.functional.conv3d(x, b.view(1, 1, 1, 7, 1), padding=(0, 3, 0))
-    x = torch.nn.functional.conv3d(x, b.view(1, 1, 1, 1, 7), padding=(0, 0, 3))
-    gt = x[0, 0] * (1.0 / max(float(b.max()) ** 3, 1e-12)) + 100.0
-    gt = gt * (spec["peak"] / float(gt.max()))
+    x = torch.nn.functional.conv3d(x, b.view(1, 1, k, 1, 1), padding=(r, 0, 0))
+    x = torch.nn.functional.conv3d(x, b.view(1, 1, 1, k, 1), padding=(0, r, 0))
+    x = torch.nn.functional.conv3d(x, b.view(1, 1, 1, 1, k), padding=(0, 0, r))
+    return x[0, 0] + background, g
+
+
+def blur_noise_torch(gt, psfs, g, bits: int = 16):
+    """V x D x H x W views of ``gt``: per-plane 'same' convolution with each
+    PSF, Poisson noise, quantised (int16 holding uint16 bits, or uint8)."""
+    import torch
+    D, H, W = gt.shape
+    V = len(psfs)
+    device = gt.device
     out = torch.empty((V, D, H, W), dtype=torch.int16 if bits == 16 else torch.uint8, device=device)
     mx = (1 << bits) - 1
-    for v, psf in enumerate(spec_psfs(spec)):
+    for v, psf in enumerate(psfs):
         kH, kW = psf.shape
         fh, fw = H + kH - 1, W + kW - 1
-        ks = torch.fft.rfft2(torch.from_numpy(psf).to(device), s=(fh, fw))
+        ks = torch.fft.rfft2(torch.from_numpy(np.ascontiguousarray(psf)).to(device), s=(fh, fw))
         for z0 in range(0, D, 32):
             z1 = min(z0 + 32, D)
             full = torch.fft.irfft2(torch.fft.rfft2(gt[z0:z1], s=(fh, fw)) * ks, s=(fh, fw))
             blurred = full[:, kH // 2:kH // 2 + H, kW // 2:kW // 2 + W].clamp_min(0)
             noisy = torch.poisson(blurred, generator=g).clamp(0, mx).round()
-            if bits == 16:
-                out[v, z0:z1] = noisy.to(torch.int32).to(torch.int16)
-            else:
-                out[v, z0:z1] = noisy.to(torch.uint8)
+            out[v, z0:z1] = noisy.to(torch.int32).to(torch.int16) if bits == 16 else noisy.to(torch.uint8)
     return out
+
+
+def views_torch(spec: dict, device="cuda", bits: int = 16, bead_density: float = 5e-5):
+    """V x D x H x W views of one volume on the GPU (torch int16 holding
+    uint16 bits for 16-bit samples, uint8 otherwise)."""
+    gt, g = bead_volume_torch(spec["D"], spec["H"], spec["W"], spec["seed"], device, bead_density)
+    gt = (gt - 100.0) * (spec["peak"] / float((gt - 100.0).max().clamp_min(1e-6))) * 0.9 + 0.1 * spec["peak"]
+    return blur_noise_torch(gt, spec_psfs(spec), g, bits)
+
+
+def warm_start_views_torch(D, H=512, W=512, views=4, seed=0, ksize=17, sigma=(1.5, 4.0), device="cuda"):
+    """Training and test planes of the learned warm start: the small plain-RL
+    generator (beads of width 1 voxel, amplitude U[500, 2000] on background
+    100; 17 x 17 PSFs of sigma 1.5 x 4.0 px; Poisson noise; uint16) at
+    H x W with ``views`` PSF orientations 180 v / views degrees.  Returns
+    (views V x D x H x W int16, ground truth D x H x W float32, PSFs)."""
+    psfs = [gaussian_psf(ksize, ksize, sigma[0], sigma[1], 180.0 * v / views) for v in range(views)]
+    density = 200.0 / (256 * 256 * 64)
+    gt, g = bead_volume_torch(D, H, W, seed, device, density)
+    return blur_noise_torch(gt, psfs, g), gt, psfs

@@ -136,6 +136,35 @@ int fmvd_b200_conv_bf16(const void *d_in, const void *d_weight, int N, int H, in
 int fmvd_b200_conv_wgrad_bf16(const void *d_grad, const void *d_in, int N, int H, int W, int cin, int cout, int taps,
                               float *d_dw, int *d_status, void *stream);
 
+/* ---- learned warm start --------------------------------------------------- */
+/* A 2-D U-Net (4 levels, base 32 channels, 3 x 3 convolutions, ReLU; BF16
+ * weights and activations, FP32 accumulation on the tensor cores) mapping
+ * the V registered view planes of a z-plane (uint16, view v of plane z at
+ * d_views + v * view_stride + z * H * W) and their mean to an estimate of
+ * the plane (float, H x W per plane).  Trained by fmvd_b200_unet_train_step
+ * (L1 loss against a target estimate, Adam) on pairs the RL iteration
+ * produces; its estimate starts RL through fmvd_b200_pad_estimate and
+ * fmvd_b200_deconvolve_device_from.  Planes: height a multiple of 64 (at
+ * least 128), width 128, 256, 512 or a multiple of 1024; 1 to 6 views. */
+typedef struct fmvd_b200_unet fmvd_b200_unet;
+fmvd_b200_unet *fmvd_b200_unet_create(int H, int W, int views, int max_batch, unsigned seed);
+void fmvd_b200_unet_destroy(fmvd_b200_unet *net);
+/* FP32 parameters, per layer weights [cout][taps][cin] then biases. */
+size_t fmvd_b200_unet_param_count(const fmvd_b200_unet *net);
+int fmvd_b200_unet_get_params(const fmvd_b200_unet *net, float *h_params);
+int fmvd_b200_unet_set_params(fmvd_b200_unet *net, const float *h_params);
+/* Gradients of the last training step (lr = 0 computes them without an update). */
+int fmvd_b200_unet_get_grads(const fmvd_b200_unet *net, float *h_grads);
+/* Estimates of nplanes planes (any count; processed in batches). Asynchronous. */
+int fmvd_b200_unet_forward(fmvd_b200_unet *net, const void *d_views, size_t view_stride, int nplanes,
+                           float *d_estimate, void *stream);
+/* One step on a batch of at most max_batch planes; *h_loss receives the
+ * mean L1 loss (in units of the per-plane scale).  Synchronous. */
+int fmvd_b200_unet_train_step(fmvd_b200_unet *net, const void *d_views, size_t view_stride, int nplanes,
+                              const float *d_target, float lr, float *h_loss, void *stream);
+/* Synchronises and reports whether a tensor-core wait timed out. */
+int fmvd_b200_unet_check(fmvd_b200_unet *net);
+
 /* ---- instrumentation ----------------------------------------------------- */
 /* Number of kernel launches the library has issued in this process. */
 unsigned long long fmvd_b200_launch_count(void);
