@@ -62,6 +62,12 @@ def parse():
     p.add_argument("--small", action="store_true", help="small volume for profiler captures")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--workload", default="transform_rl", choices=["transform_rl", "warmstart"],
+                   help="warmstart: learned warm start vs plain RL-50 (time to the RL-50 result)")
+    p.add_argument("--train-planes", type=int, default=4000)
+    p.add_argument("--epochs", type=int, default=12)
+    p.add_argument("--target-iterations", type=int, default=42,
+                   help="warm start: RL iterations of the training targets (the network then needs 50 - this)")
     return p.parse_args()
 
 
@@ -434,10 +440,94 @@ def run_reference(args):
     }), flush=True)
 
 
+def unet_flops_per_plane(H, W, V=4, base=32):
+    """Multiply-add FLOPs (x 2) of one plane through the network's
+    convolutions: forward, and forward + data + weight gradients."""
+    shapes = [(64, base, 1), (base, base, 9)]
+    for l in range(1, 4):
+        shapes += [(base << (l - 1), base << l, 9), (base << l, base << l, 9)]
+    for l in (2, 1, 0):
+        shapes += [(base << (l + 1), base << l, 9), (base << l, base << l, 9)]
+    levels = [0, 0] + [l for l in range(1, 4) for _ in (0, 1)] + [l for l in (2, 1, 0) for _ in (0, 1)]
+    fwd = train = 0.0
+    for i, ((cin, cout, taps), l) in enumerate(zip(shapes, levels)):
+        f = 2.0 * (H >> l) * (W >> l) * cout * taps * cin
+        fwd += f
+        train += f * (2 if i == 0 else 3)
+    return fwd, train
+
+
+def run_warmstart(args):
+    """Learned warm start (a 2-D U-Net on the tensor cores) vs plain RL-50 on
+    512 x 512 planes of 4 views: train on plain RL-50 targets, tune k so that
+    warm start + RL-k is within 1e-2 relative L2 of plain RL-50 on held-out
+    planes, then time both paths to the RL-50 result on test planes."""
+    import torch
+    from gpu_deconvolution_b200 import api
+    from gpu_deconvolution_b200 import warmstart as WS
+    H = W = 512
+    V, N_RL, TOL = 4, 50, 1e-2
+    n_train = args.train_planes
+    t0 = time.perf_counter()
+    views, targets, gt, psfs = WS.training_pairs(n_train, H, W, V, args.target_iterations, seed=1000,
+                                                 planes_per_volume=64)
+    t_data = time.perf_counter() - t0
+    tv, tt, tg, _ = WS.training_pairs(64, H, W, V, N_RL, seed=900000, planes_per_volume=64)   # k tuning
+    ev, et, eg, _ = WS.training_pairs(64, H, W, V, N_RL, seed=950000, planes_per_volume=64)   # test
+    net = WS.WarmStartNet(H, W, V, max_batch=16, seed=0)
+    plan = api.DevicePlan(H, W, WS.equal_weights(H, W, V), [p.copy() for p in psfs], 0)
+    # training (timed on the device, steps of 16 planes)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    hist = WS.train(net, views, targets, epochs=args.epochs, batch=16, lr=1e-3,
+                    log=lambda m: print(m, file=sys.stderr, flush=True))
+    e1.record()
+    torch.cuda.synchronize()
+    t_train = e0.elapsed_time(e1) / 1e3
+    steps = args.epochs * (n_train // 16)
+    fwd_f, train_f = unet_flops_per_plane(H, W, V)
+    del views, targets, gt
+    torch.cuda.empty_cache()
+    k, k_errors = WS.tune_k(net, plan, tv, tt, TOL,
+                            candidates=tuple(range(0, 13)) + (14, 16, 20, 25, 30, 40))
+    kk = k if k is not None else N_RL
+    # time to the RL-50 result on the test planes
+    t_plain = WS.time_cuda(lambda: WS.rl_planes(plan, ev, N_RL))
+    t_warm = WS.time_cuda(lambda: WS.warm_deconvolve(net, plan, ev, kk))
+    t_net = WS.time_cuda(lambda: net.forward(ev))
+    warm, _ = WS.warm_deconvolve(net, plan, ev, kk)
+    plain, _ = WS.rl_planes(plan, ev, N_RL)
+    err = WS.rel_l2_planes(warm.contiguous(), et)
+    psnr_plain = WS.psnr(plain, eg)
+    psnr_warm = WS.psnr(warm, eg)
+    net.check()
+    line = {
+        "metric": "time to the plain RL-50 result, warm start vs plain", "unit": "ms per 64 planes",
+        "value": t_warm, "plain_rl50_ms": t_plain, "speedup": t_plain / t_warm, "k": k,
+        "rel_l2_vs_rl50": {"max": float(err.max()), "mean": float(err.mean()), "tolerance": TOL},
+        "psnr_db": {"plain_rl50": psnr_plain, "warm": psnr_warm, "delta": psnr_warm - psnr_plain},
+        "k_search": {str(a): b for a, b in k_errors.items()},
+        "network_ms_per_64_planes": t_net,
+        "network_tflops": fwd_f * 64 / (t_net / 1e3) / 1e12,
+        "training": {"planes": n_train, "target_rl_iterations": args.target_iterations, "epochs": args.epochs,
+                     "batch": 16, "steps": steps, "seconds": t_train,
+                     "tflops": train_f * 16 * steps / t_train / 1e12, "loss_per_epoch": hist,
+                     "data_seconds": t_data},
+        "dtype": "bf16 network (fp32 accumulation), f32 RL", "data": "synthetic",
+        "config": {"workload": "learned warm start: 4 views u16 512x512 planes, 17x17 PSFs sigma 1.5x4.0, "
+                               "plain RL-50 targets, U-Net 4 levels base 32", "fft_plane": [plan.fftH, plan.fftW]},
+    }
+    print(json.dumps(line), flush=True)
+    plan.destroy()
+    net.destroy()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "warmstart":
+        run_warmstart(args)
     else:
         run_b200(args)
 

@@ -222,11 +222,13 @@ class DevicePlan:
         if r != 0:
             raise FmvdError(name + " failed")
 
-    def pad_estimate(self, planes, out, stream=0):
+    def pad_estimate(self, planes, out, floor=float("-inf"), stream=0):
         """Data-plane float estimates (D x dataH x dataW CUDA tensor) onto the
-        FFT plane (``out``: D x fftH x fftW) with the views' border padding."""
+        FFT plane (``out``: D x fftH x fftW) with the views' border padding,
+        raised to ``floor``."""
         native.clear_errors()
-        r = self.lib.fmvd_b200_pad_estimate(self.plan, planes.data_ptr(), out.data_ptr(), planes.shape[0], stream)
+        r = self.lib.fmvd_b200_pad_estimate(self.plan, planes.data_ptr(), out.data_ptr(), planes.shape[0],
+                                            float(floor), stream)
         native.check("fmvd_b200_pad_estimate")
         if r != 0:
             raise FmvdError("fmvd_b200_pad_estimate failed")

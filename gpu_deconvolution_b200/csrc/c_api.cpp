@@ -149,13 +149,14 @@ int fmvd_b200_deconvolve_device_from(fmvd_b200_plan *plan, const void *d_views, 
                : 1;
 }
 
-int fmvd_b200_pad_estimate(const fmvd_b200_plan *plan, const float *d_in, float *d_out, int nplanes, void *stream)
+int fmvd_b200_pad_estimate(const fmvd_b200_plan *plan, const float *d_in, float *d_out, int nplanes,
+                           float floor_value, void *stream)
 {
     if (!plan || nplanes < 0 || (nplanes > 0 && (!d_in || !d_out))) {
         fmvd::report_error("fmvd: invalid arguments to fmvd_b200_pad_estimate");
         return 1;
     }
-    return fmvd::pad_estimate(d_in, d_out, nplanes, plan->eng->dims, (cudaStream_t)stream) ? 0 : 1;
+    return fmvd::pad_estimate(d_in, d_out, nplanes, plan->eng->dims, floor_value, (cudaStream_t)stream) ? 0 : 1;
 }
 
 int fmvd_b200_plane_stats(const float *d_a, const float *d_b, int nplanes, int H, int W, int rows, int cols,

@@ -86,7 +86,7 @@ Engine *plan_engine_8(const fmvd_plan_cuda_8 *p);
 // ---- convergence statistics and warm-start padding (stats.cu)
 bool plane_stats(const float *a, const float *b, int nplanes, int H, int W, int rows, int cols, double *out,
                  cudaStream_t s);
-bool pad_estimate(const float *in, float *out, int nplanes, const RlDims &d, cudaStream_t s);
+bool pad_estimate(const float *in, float *out, int nplanes, const RlDims &d, float floor_value, cudaStream_t s);
 
 // ---- resampler (transform.cu)
 void transform_file(int bits, const void *const *h_planes, int w, int h, int d, int tw, int th, int td,

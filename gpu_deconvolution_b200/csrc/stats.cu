@@ -70,9 +70,10 @@ __device__ __forceinline__ int clamp_index(int i, int n, int border)
 
 // Data-plane float estimates (dataH x dataW) onto the H x W FFT plane with
 // the clamp-to-border padding the data receives (rows beyond dataH + byD and
-// columns beyond dataW + bxD wrap to row / column 0).
+// columns beyond dataW + bxD wrap to row / column 0), raised to floor_value
+// (the multiplicative RL update needs a positive estimate).
 __global__ void pad_estimate_kernel(const float *__restrict__ in, float *__restrict__ out, int H, int W, int dataH,
-                                    int dataW, int byD, int bxD)
+                                    int dataW, int byD, int bxD, float floor_value)
 {
     const int p = blockIdx.z;
     const int y = blockIdx.y;
@@ -80,7 +81,7 @@ __global__ void pad_estimate_kernel(const float *__restrict__ in, float *__restr
     const float *src = in + ((size_t)p * dataH + sy) * dataW;
     float *dst = out + ((size_t)p * H + y) * W;
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < W; x += gridDim.x * blockDim.x)
-        dst[x] = __ldg(src + clamp_index(x, dataW, bxD));
+        dst[x] = fmaxf(__ldg(src + clamp_index(x, dataW, bxD)), floor_value);
 }
 
 } // namespace
@@ -95,7 +96,7 @@ bool plane_stats(const float *a, const float *b, int nplanes, int H, int W, int 
     return FMVD_CHECK(cudaGetLastError());
 }
 
-bool pad_estimate(const float *in, float *out, int nplanes, const RlDims &d, cudaStream_t s)
+bool pad_estimate(const float *in, float *out, int nplanes, const RlDims &d, float floor_value, cudaStream_t s)
 {
     if (nplanes <= 0)
         return true;
@@ -106,7 +107,7 @@ bool pad_estimate(const float *in, float *out, int nplanes, const RlDims &d, cud
         const dim3 grid((d.W + threads - 1) / threads, d.H, n);
         pad_estimate_kernel<<<grid, threads, 0, s>>>(in + (size_t)p0 * d.dataH * d.dataW,
                                                      out + (size_t)p0 * d.H * d.W, d.H, d.W, d.dataH, d.dataW,
-                                                     d.byD, d.bxD);
+                                                     d.byD, d.bxD, floor_value);
         rl_count_launch(1);
     }
     return FMVD_CHECK(cudaGetLastError());

@@ -152,13 +152,17 @@ def training_pairs(n_planes: int, H: int = 512, W: int = 512, views: int = 4, it
 
 
 def train(net: WarmStartNet, views, targets, epochs: int = 10, batch: int = 16, lr: float = 1e-3, seed: int = 0,
-          log=None):
-    """Adam on the L1 loss over shuffled batches; returns the per-epoch mean
-    losses."""
+          log=None, final_lr_fraction: float = 0.02):
+    """Adam on the L1 loss over shuffled batches, the step size decaying on a
+    cosine from ``lr`` to ``final_lr_fraction * lr``; returns the per-epoch
+    mean losses."""
     import torch
     V, N, H, W = views.shape
     rng = np.random.default_rng(seed)
     history = []
+    per_epoch = max(1, N // batch)
+    total = max(1, epochs * per_epoch - 1)
+    step = 0
     for ep in range(epochs):
         order = rng.permutation(N)
         losses = []
@@ -166,7 +170,9 @@ def train(net: WarmStartNet, views, targets, epochs: int = 10, batch: int = 16, 
             idx = torch.from_numpy(order[b0:b0 + batch]).to(views.device)
             bv = views.index_select(1, idx).contiguous()
             bt = targets.index_select(0, idx).contiguous()
-            losses.append(net.train_step(bv, bt, lr))
+            f = final_lr_fraction + (1.0 - final_lr_fraction) * 0.5 * (1.0 + np.cos(np.pi * step / total))
+            losses.append(net.train_step(bv, bt, lr * f))
+            step += 1
         history.append(float(np.mean(losses)))
         if log:
             log(f"epoch {ep}: loss {history[-1]:.5f}")
@@ -181,8 +187,9 @@ def rel_l2_planes(a, b):
 
 
 def warm_deconvolve(net: WarmStartNet, plan: api.DevicePlan, views, k: int, check_tol: float | None = None,
-                    fallback_iterations: int = 50):
-    """Network estimate -> padding -> k RL iterations.  With ``check_tol``,
+                    fallback_iterations: int = 50, floor: float = 1.0):
+    """Network estimate -> padding (values below ``floor`` samples raised to
+    it: RL needs a positive start) -> k RL iterations.  With ``check_tol``,
     planes whose estimate still changes by more than check_tol (relative L2
     over one more iteration, FP64 sums) are redone with plain RL.  Returns
     (data-plane estimates N x H x W, indices of planes that fell back)."""
@@ -190,7 +197,7 @@ def warm_deconvolve(net: WarmStartNet, plan: api.DevicePlan, views, k: int, chec
     V, N, H, W = views.shape
     guess = net.forward(views)
     init = torch.empty((N, plan.fftH, plan.fftW), dtype=torch.float32, device=views.device)
-    plan.pad_estimate(guess, init)
+    plan.pad_estimate(guess, init, floor)
     est, padded = rl_planes(plan, views, k, init=init)
     fell_back = np.zeros(0, np.int64)
     if check_tol is not None:

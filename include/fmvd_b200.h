@@ -49,8 +49,10 @@ int fmvd_b200_deconvolve_device_from(fmvd_b200_plan *plan, const void *d_views, 
                                      void *stream);
 /* Estimates on the data plane (nplanes x dataH x dataW floats) onto the FFT
  * plane (nplanes x fftH x fftW) with the clamp-to-border padding the views
- * receive: the initial estimate of a warm start. */
-int fmvd_b200_pad_estimate(const fmvd_b200_plan *plan, const float *d_in, float *d_out, int nplanes, void *stream);
+ * receive, values below floor_value raised to it (RL's multiplicative update
+ * needs a positive estimate): the initial estimate of a warm start. */
+int fmvd_b200_pad_estimate(const fmvd_b200_plan *plan, const float *d_in, float *d_out, int nplanes,
+                           float floor_value, void *stream);
 /* Convergence check: per plane p of nplanes H x W float planes, in FP64 over
  * rows < rows and columns < cols, d_stats[4p..4p+3] = sum a, sum a^2,
  * sum (a - b)^2, sum |a - b| (d_b may be null: the last two are 0).
