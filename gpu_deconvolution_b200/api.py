@@ -272,6 +272,50 @@ class DevicePlan:
             pass
 
 
+class Reconstructor:
+    """Host source volumes -> resampling -> plain RL -> host result, with the
+    resampled frame kept on the device (fmvd_b200_reconstruct_host).
+    ``plan`` is a DevicePlan for the frame's th x tw planes and V views."""
+
+    def __init__(self, plan, views: int, src_shape, frame, chunk_planes: int = 0):
+        self.lib = native.load()
+        d, h, w = src_shape
+        td, th, tw = frame
+        self.plan, self.V, self.src_shape, self.frame = plan, views, tuple(src_shape), tuple(frame)
+        native.clear_errors()
+        self.rec = self.lib.fmvd_b200_reconstructor_create(plan.plan, views, w, h, d, tw, th, td, int(chunk_planes))
+        native.check("fmvd_b200_reconstructor_create")
+        if not self.rec:
+            raise FmvdError("reconstructor creation failed")
+
+    def run(self, views, inverses, iterations: int, out: np.ndarray | None = None) -> np.ndarray:
+        """views: V host arrays d x h x w (uint16 or uint8, contiguous);
+        inverses: V 3x4 target->source matrices."""
+        vs = [np.ascontiguousarray(v) for v in views]
+        assert len(vs) == self.V and all(v.shape == self.src_shape for v in vs)
+        m = np.ascontiguousarray(np.stack([np.asarray(x, np.float32).reshape(12) for x in inverses]))
+        if out is None:
+            out = np.empty(self.frame, vs[0].dtype)
+        ptrs = (C.c_void_p * self.V)(*[v.ctypes.data for v in vs])
+        native.clear_errors()
+        r = self.lib.fmvd_b200_reconstruct_host(self.rec, ptrs, m.ctypes.data, int(iterations), out.ctypes.data)
+        native.check("fmvd_b200_reconstruct_host")
+        if r != 0:
+            raise FmvdError("fmvd_b200_reconstruct_host failed")
+        return out
+
+    def destroy(self):
+        if self.rec:
+            self.lib.fmvd_b200_reconstructor_destroy(self.rec)
+            self.rec = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
 class Batch:
     """Several device-resident volumes (each with its own ``DevicePlan``)
     deconvolved by one CUDA graph launch (fmvd_b200_batch_*).  The plans and

@@ -39,6 +39,7 @@ LIB_SOURCES = [
     "noalloc.cu",
     "stats.cu",
     "batch.cpp",
+    "reconstruct.cpp",
     "unet_gemm.cu",
     "unet_capi.cpp",
     "unet_layers.cu",

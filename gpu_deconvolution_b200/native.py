@@ -103,6 +103,9 @@ SIGNATURES = {
     "fmvd_b200_unet_forward": (c_int, [c_p, c_p, C.c_size_t, c_int, c_p, c_p]),
     "fmvd_b200_unet_train_step": (c_int, [c_p, c_p, C.c_size_t, c_int, c_p, C.c_float, c_p, c_p]),
     "fmvd_b200_unet_check": (c_int, [c_p]),
+    "fmvd_b200_reconstructor_create": (c_p, [c_p, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_int]),
+    "fmvd_b200_reconstruct_host": (c_int, [c_p, c_p, c_p, c_int, c_p]),
+    "fmvd_b200_reconstructor_destroy": (None, [c_p]),
     "fmvd_b200_batch_create": (c_p, [c_int, c_p, c_p, c_p, c_p, c_p, c_p, c_int]),
     "fmvd_b200_batch_run": (c_int, [c_p, c_p]),
     "fmvd_b200_batch_branches": (c_int, [c_p]),

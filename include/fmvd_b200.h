@@ -106,6 +106,25 @@ struct fmvd_plan_cuda_8 *fmvd_b200_initialize_cuda_8(int dataH, int dataW, float
                                                      datasource_8_t get_next_plane, datasink_8_t return_next_plane,
                                                      int pairs_per_batch);
 
+/* ---- host buffers in, host buffers out ----------------------------------- */
+/* No counterpart in the reference (whose plugin path writes the resampled
+ * frame to the host and streams it back plane by plane).  A reconstructor
+ * holds the device buffers for one geometry: V source volumes of d planes of
+ * h x w samples, a td-plane frame of th x tw (the plan's data plane), work in
+ * chunks of chunk_planes target planes (0 = four plan batches). */
+typedef struct fmvd_b200_reconstructor fmvd_b200_reconstructor;
+fmvd_b200_reconstructor *fmvd_b200_reconstructor_create(fmvd_b200_plan *plan, int views, int w, int h, int d,
+                                                        int tw, int th, int td, int chunk_planes);
+/* Resamples view v (h_views[v]: d x h x w contiguous samples, target->source
+ * 3x4 matrix h_inverses + 12 v, as transform_cuda_*) into the frame and
+ * deconvolves it with the plan (iterations of plain RL); h_out receives td
+ * planes of th x tw samples.  The frame never leaves the device; result
+ * chunks are copied back while the next chunk computes.  Synchronous;
+ * sources in pinned memory upload fastest. */
+int fmvd_b200_reconstruct_host(fmvd_b200_reconstructor *rec, const void *const *h_views, const float *h_inverses,
+                               int iterations, void *h_out);
+void fmvd_b200_reconstructor_destroy(fmvd_b200_reconstructor *rec);
+
 /* ---- resampler ---------------------------------------------------------- */
 /* Row pitch (samples) that device source volumes must use. */
 size_t fmvd_b200_source_pitch(int bits, int w);
