@@ -251,6 +251,202 @@ __global__ void __launch_bounds__(128, 1)
         umma::tmem_dealloc(tmem, C::TCOLS);
 }
 
+// Persistent forward / data-gradient GEMM (mode 0 geometry).  Each CTA
+// walks tiles blockIdx.x, blockIdx.x + gridDim.x, ... of the 128-pixel x BN
+// output; the K blocks of consecutive tiles flow through one TMA stage ring
+// without a break, and the accumulator is double-buffered in tensor memory,
+// so the epilogue of a tile overlaps the MMAs of the next.  Warps 0-3: the
+// epilogue (warp w reads accumulator lanes 32w..32w+31); warp 4: tensor
+// memory allocation and, in lane 0, the TMA producer; warp 5 lane 0: the MMA
+// issuer.
+constexpr int kPersistentThreads = 192;
+
+template <int CB, int BN>
+struct PersistCfg {
+    static constexpr int R = CB * 2;
+    static constexpr uint32_t SA = 128u * R, SB = (uint32_t)BN * R;
+    static constexpr uint32_t STAGE = align1k(SA) + align1k(SB);
+    static constexpr int ACC_COLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
+    static constexpr int TCOLS = 2 * ACC_COLS;  // two accumulators
+    // one CTA per SM when its accumulators take all of tensor memory: then
+    // the stage ring may use most of shared memory
+    static constexpr uint32_t BUDGET = TCOLS == 512 ? 196608u : 98304u;
+    static constexpr int STAGES = BUDGET / STAGE >= 6 ? 6 : (BUDGET / STAGE >= 2 ? (int)(BUDGET / STAGE) : 2);
+    static constexpr uint32_t SMEM = STAGES * STAGE + 1024;
+    static constexpr int KSTEPS = CB / 16;
+};
+
+template <int CB, int BN>
+__global__ void __launch_bounds__(kPersistentThreads, 1)
+    conv_gemm_persistent(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                         const GemmArgs g, int ntiles, int ntiles_n)
+{
+    using C = PersistCfg<CB, BN>;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ __align__(8) uint64_t full[C::STAGES], empty[C::STAGES], acc_full[2], acc_empty[2];
+    __shared__ uint32_t tmem_sh;
+    __shared__ int fail_store;
+    volatile int &fail_sh = fail_store;  // set by any role that gave up waiting
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tx = g.W / g.bw, ty = g.H / g.bh;
+    const int nk = g.taps * (g.cin / CB);
+    const int cblocks = g.cin / CB;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < C::STAGES; i++) {
+            umma::bar_init(&full[i], 1);
+            umma::bar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < 2; i++) {
+            umma::bar_init(&acc_full[i], 1);
+            umma::bar_init(&acc_empty[i], 4);  // one arrival per epilogue warp
+        }
+        umma::bar_fence_init();
+        fail_sh = 0;
+    }
+    if (warp == 4) {
+        umma::tmem_alloc(&tmem_sh, C::TCOLS);
+        umma::tmem_relinquish();
+    }
+    umma::tc_fence_before();
+    __syncthreads();
+    umma::tc_fence_after();
+    const uint32_t tmem = tmem_sh;
+
+    auto tile_coords = [&](int tile, int &n, int &y0, int &x0, int &co0) {
+        const int tp = tile / ntiles_n, tn = tile % ntiles_n;
+        n = tp / (tx * ty);
+        const int r = tp % (tx * ty);
+        y0 = (r / tx) * g.bh;
+        x0 = (r % tx) * g.bw;
+        co0 = tn * BN;
+    };
+
+    if (warp == 4) {
+        if (lane == 0) {
+            // ---- producer
+            int gk = 0;
+            for (int tile = blockIdx.x; tile < ntiles && !fail_sh; tile += gridDim.x) {
+                int n, y0, x0, co0;
+                tile_coords(tile, n, y0, x0, co0);
+                for (int kb = 0; kb < nk; kb++, gk++) {
+                    const int s = gk % C::STAGES, round = gk / C::STAGES;
+                    if (round > 0 && !umma::bar_wait(&empty[s], (round - 1) & 1)) {
+                        fail_sh = 1;
+                        break;
+                    }
+                    umma::bar_expect_tx(&full[s], C::SA + C::SB);
+                    uint8_t *a = smem + s * C::STAGE;
+                    uint8_t *b = a + align1k(C::SA);
+                    const int t = kb / cblocks, cb = kb % cblocks;
+                    int dy, dx;
+                    tap_offset(g.taps, t, dy, dx);
+                    umma::tma_load_4d(a, &tmA, cb * CB, x0 + dx, y0 + dy, n, &full[s]);
+                    umma::tma_load_2d(b, &tmB, kb * CB, co0, &full[s]);
+                }
+            }
+        }
+    } else if (warp == 5) {
+        if (lane == 0) {
+            // ---- MMA issue
+            const uint32_t idesc = umma::make_idesc(128, BN, 0, 0);
+            int gk = 0, it = 0;
+            for (int tile = blockIdx.x; tile < ntiles && !fail_sh; tile += gridDim.x, it++) {
+                const int ab = it & 1;
+                if (it >= 2 && !umma::bar_wait(&acc_empty[ab], ((it >> 1) - 1) & 1)) {
+                    fail_sh = 1;
+                    break;
+                }
+                umma::tc_fence_after();
+                const uint32_t acc = tmem + ab * C::ACC_COLS;
+                for (int kb = 0; kb < nk; kb++, gk++) {
+                    const int s = gk % C::STAGES, round = gk / C::STAGES;
+                    if (!umma::bar_wait(&full[s], round & 1)) {
+                        fail_sh = 1;
+                        break;
+                    }
+                    umma::tc_fence_after();
+                    const uint32_t a0 = umma::smem_addr(smem + s * C::STAGE);
+                    const uint32_t b0 = a0 + align1k(C::SA);
+#pragma unroll
+                    for (int kk = 0; kk < C::KSTEPS; kk++) {
+                        const uint64_t ad = umma::make_desc(a0 + kk * 32, 16, 8 * C::R, C::R);
+                        const uint64_t bd = umma::make_desc(b0 + kk * 32, 16, 8 * C::R, C::R);
+                        umma::mma_bf16(acc, ad, bd, idesc, (kb > 0 || kk > 0) ? 1u : 0u);
+                    }
+                    umma::mma_commit(&empty[s]);
+                }
+                umma::mma_commit(&acc_full[ab]);
+            }
+        }
+    } else {
+        // ---- epilogue: warp w owns accumulator rows 32w..32w+31
+        const int row = warp * 32 + lane;
+        int it = 0;
+        for (int tile = blockIdx.x; tile < ntiles && !fail_sh; tile += gridDim.x, it++) {
+            const int ab = it & 1;
+            if (!umma::bar_wait(&acc_full[ab], (it >> 1) & 1)) {
+                fail_sh = 1;
+                break;
+            }
+            umma::tc_fence_after();
+            int n, y0, x0, co0;
+            tile_coords(tile, n, y0, x0, co0);
+            const int y = y0 + row / g.bw, x = x0 + row % g.bw;
+            const size_t pix = ((size_t)n * g.H + y) * g.W + x;
+            const uint32_t trow = tmem + ab * C::ACC_COLS + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                float v[16];
+                umma::tmem_ld16(trow + c0, v);
+                const int co = co0 + c0;
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    float t = v[i];
+                    if (g.bias)
+                        t += g.bias[co + i];
+                    if (g.add)
+                        t += __bfloat162float(g.add[pix * g.add_ld + co + i]);
+                    if (g.relu)
+                        t = fmaxf(t, 0.f);
+                    if (g.mask && !(__bfloat162float(g.mask[pix * g.mask_ld + co + i]) > 0.f))
+                        t = 0.f;
+                    v[i] = t;
+                }
+                if (g.out) {
+                    __align__(16) bf16 h[16];
+#pragma unroll
+                    for (int i = 0; i < 16; i++)
+                        h[i] = __float2bfloat16_rn(v[i]);
+                    uint4 *dst = reinterpret_cast<uint4 *>(g.out + pix * g.out_ld + g.out_coff + co);
+                    dst[0] = reinterpret_cast<const uint4 *>(h)[0];
+                    dst[1] = reinterpret_cast<const uint4 *>(h)[1];
+                }
+                if (g.out_f32) {
+                    float4 *dst = reinterpret_cast<float4 *>(g.out_f32 + pix * g.outf_ld + co);
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+                        dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                }
+            }
+            umma::tc_fence_before();
+            __syncwarp();
+            if (lane == 0)
+                umma::bar_arrive(&acc_empty[ab]);
+        }
+    }
+    __syncwarp();
+    umma::tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && fail_sh && g.status)
+        atomicExch(g.status, 1);
+    if (warp == 4) {
+        umma::tc_fence_after();
+        umma::tmem_dealloc(tmem, C::TCOLS);
+    }
+}
+
 // ------------------------------------------------------------------ host
 namespace {
 
@@ -320,7 +516,48 @@ void pixel_box(int W, int count, int &bw, int &bh)
     bh = count / bw;
 }
 
+template <int CB, int BN>
+bool launch_persistent(const CUtensorMap &ta, const CUtensorMap &tb, const GemmArgs &g, int ntiles, int ntiles_n,
+                       cudaStream_t s)
+{
+    using C = PersistCfg<CB, BN>;
+    auto k = conv_gemm_persistent<CB, BN>;
+    static int sms = 0;
+    static bool configured = false;
+    if (!configured) {
+        int dev = 0;
+        if (!FMVD_CHECK(cudaGetDevice(&dev)) ||
+            !FMVD_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) ||
+            !FMVD_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM)))
+            return false;
+        configured = true;
+    }
+    // CTAs per SM: tensor memory (512 columns) and shared memory allow
+    const int by_tmem = 512 / C::TCOLS;
+    const int by_smem = (int)(200u * 1024u / C::SMEM);
+    const int per_sm = by_tmem < by_smem ? by_tmem : by_smem;
+    int grid = sms * (per_sm < 1 ? 1 : per_sm);
+    if (grid > ntiles)
+        grid = ntiles;
+    k<<<grid, kPersistentThreads, C::SMEM, s>>>(ta, tb, g, ntiles, ntiles_n);
+    rl_count_launch(1);
+    return FMVD_CHECK(cudaGetLastError());
+}
+
 #define FMVD_BN_CASES(F) F(16) F(32) F(64) F(128) F(256)
+
+template <int CB>
+bool dispatch_persistent(int bn, const CUtensorMap &ta, const CUtensorMap &tb, const GemmArgs &g, int ntiles,
+                         int ntiles_n, cudaStream_t s)
+{
+    switch (bn) {
+#define X(B) \
+    case B: return launch_persistent<CB, B>(ta, tb, g, ntiles, ntiles_n, s);
+        FMVD_BN_CASES(X)
+#undef X
+    default: report_error("fmvd: unsupported GEMM N tile"); return false;
+    }
+}
 
 template <int MODE, int CBA, int CBB>
 bool dispatch_bn(int bn, const CUtensorMap &ta, const CUtensorMap &tb, const GemmArgs &g, dim3 grid, cudaStream_t s)
@@ -379,8 +616,16 @@ bool conv_forward(const ConvDesc &c, cudaStream_t s)
     g.mask_ld = c.mask_ld ? c.mask_ld : c.cout;
     g.relu = c.relu;
     g.status = c.status;
-    const dim3 grid((unsigned)(c.N * (c.H / bh) * (c.W / bw)), (unsigned)(c.cout / bn), 1);
-    return cb == 64 ? dispatch_bn<0, 64, 64>(bn, ta, tb, g, grid, s) : dispatch_bn<0, 32, 32>(bn, ta, tb, g, grid, s);
+    const int ntiles_n = c.cout / bn;
+    const int ntiles = c.N * (c.H / bh) * (c.W / bw) * ntiles_n;
+    if (cb == 32 && bn <= 32) {
+        // 32-channel operands with a narrow N: one CTA per tile keeps more
+        // K blocks in flight per SM (measured faster on B200)
+        const dim3 grid((unsigned)(ntiles / ntiles_n), (unsigned)ntiles_n, 1);
+        return dispatch_bn<0, 32, 32>(bn, ta, tb, g, grid, s);
+    }
+    return cb == 64 ? dispatch_persistent<64>(bn, ta, tb, g, ntiles, ntiles_n, s)
+                    : dispatch_persistent<32>(bn, ta, tb, g, ntiles, ntiles_n, s);
 }
 
 bool conv_wgrad(const WgradDesc &c, cudaStream_t s)

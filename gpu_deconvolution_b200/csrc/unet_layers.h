@@ -10,6 +10,11 @@ namespace unet {
 
 constexpr int kInputChannels = 64;   // first-layer patch channels: 9 taps x (views + mean), zero padded
 constexpr int kMaxOutChannels = 64;  // channels feeding the 1x1 output layer
+constexpr int kScaleParts = 64;      // fixed parts of the per-plane scale reduction
+
+// Channel counts of the layer kernels are multiples of 8 (16-byte vectors),
+// at most 256.  plane_scale: scale holds N * (kScaleParts + 1) floats, the
+// first N receive the scales.
 
 bool plane_scale(const unsigned short *views, size_t view_stride, int V, int N, int HW, float *scale, cudaStream_t s);
 bool input_patches(const unsigned short *views, size_t view_stride, int V, int N, int H, int W, const float *scale,

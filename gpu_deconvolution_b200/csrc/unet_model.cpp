@@ -277,7 +277,7 @@ Net *create(int H, int W, int V, int maxN, unsigned seed)
     for (const Layer &l : n->L)
         wtotal += 2 * (size_t)l.cout * l.taps * l.cin;
     bool ok = dalloc(*n, &n->params, off) && dalloc(*n, &n->grads, off) && dalloc(*n, &n->m, off) &&
-              dalloc(*n, &n->v, off) && dalloc(*n, &n->wbuf, wtotal) && dalloc(*n, &n->scale, maxN) &&
+              dalloc(*n, &n->v, off) && dalloc(*n, &n->wbuf, wtotal) && dalloc(*n, &n->scale, (size_t)maxN * (kScaleParts + 1)) &&
               dalloc(*n, &n->gy, (size_t)maxN * H * W) && dalloc(*n, &n->loss, 1) && dalloc(*n, &n->status, 1);
     if (ok) {
         bf16 *w = n->wbuf;
