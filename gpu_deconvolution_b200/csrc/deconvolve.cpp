@@ -111,7 +111,7 @@ typename Traits<S>::plan_t *initialize(int dataH, int dataW, const float *const 
         return nullptr;
     }
     Engine *e = engine_create(Traits<S>::bits, dataH, dataW, h_Weights, h_Kernel, kernelH, kernelW, type, nViews,
-                              pairs_cap);
+                              pairs_cap, 0, 1);
     if (!e)
         return nullptr;
     Plan<S> *p = new Plan<S>();

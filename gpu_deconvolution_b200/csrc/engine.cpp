@@ -159,12 +159,13 @@ unsigned g_constants_uploaded = 0;
 
 } // namespace
 
-int default_pairs_cap(int H, int W)
+int default_pairs_cap(int H, int W, int lanes)
 {
-    // Keep the batch's complex work planes around 48 MB so that they stay
-    // resident in the 126 MB L2 between passes.
+    // Keep the complex work planes of the batches in flight (one per lane)
+    // around 48 MB in total so that they stay resident in the 126 MB L2
+    // between passes.
     const size_t per_pair = (size_t)H * W * sizeof(float2);
-    size_t cap = ((size_t)48 << 20) / per_pair;
+    size_t cap = ((size_t)48 << 20) / per_pair / (size_t)(lanes > 1 ? lanes : 1);
     if (cap < 1)
         cap = 1;
     if (cap > 64)
@@ -173,7 +174,7 @@ int default_pairs_cap(int H, int W)
 }
 
 Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weights, float **h_Kernel, int kH,
-                      int kW, int psf_type, int nViews, int pairs_cap, int col_warps)
+                      int kW, int psf_type, int nViews, int pairs_cap, int col_warps, int lanes)
 {
     if (bits != 8 && bits != 16) {
         report_error("fmvd: unsupported sample size");
@@ -224,7 +225,8 @@ Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weig
     e->kH = kH;
     e->kW = kW;
     e->device = dev;
-    e->pairs_cap = pairs_cap > 0 ? pairs_cap : default_pairs_cap(H, W);
+    e->lanes = lanes > 1 ? 2 : 1;
+    e->pairs_cap = pairs_cap > 0 ? pairs_cap : default_pairs_cap(H, W, e->lanes);
     e->spec_elems = rl_spectrum_elems(H, W);
 
     // kernel 2 from the unnormalised kernels, then normalise the caller's kernels
@@ -244,6 +246,12 @@ Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weig
               FMVD_CHECK(cudaMalloc(&e->twH, sizeof(float2) * H)) && FMVD_CHECK(cudaMalloc(&e->twW, sizeof(float2) * W)) &&
               FMVD_CHECK(cudaMalloc(&e->wtwH, sizeof(float2) * H)) && FMVD_CHECK(cudaMalloc(&e->wtwW, sizeof(float2) * W)) &&
               FMVD_CHECK(cudaMalloc(&e->status, sizeof(int))) && FMVD_CHECK(cudaMemset(e->status, 0, sizeof(int)));
+    if (ok && e->lanes == 2)
+        ok = FMVD_CHECK(cudaMalloc(&e->C2, sizeof(float2) * (size_t)H * W * e->pairs_cap)) &&
+             FMVD_CHECK(cudaMalloc(&e->est2, sizeof(float2) * (size_t)H * W * e->pairs_cap)) &&
+             FMVD_CHECK(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking)) &&
+             FMVD_CHECK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming)) &&
+             FMVD_CHECK(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
     if (!ok) {
         engine_destroy(e);
         return nullptr;
@@ -321,6 +329,14 @@ void engine_destroy(Engine *e)
     cudaFree(e->wtwH);
     cudaFree(e->wtwW);
     cudaFree(e->status);
+    cudaFree(e->C2);
+    cudaFree(e->est2);
+    if (e->side)
+        cudaStreamDestroy(e->side);
+    if (e->ev_fork)
+        cudaEventDestroy(e->ev_fork);
+    if (e->ev_join)
+        cudaEventDestroy(e->ev_join);
     delete e;
 }
 
@@ -380,17 +396,33 @@ bool engine_run(Engine *e, const void *data, size_t view_stride, void *out, int 
                 float *est_out, cudaStream_t s, const float *init)
 {
     const size_t plane = (size_t)e->dims.dataH * e->dims.dataW;
+    const size_t fplane = (size_t)e->dims.H * e->dims.W;
     const size_t es = e->dims.bits == 16 ? 2 : 1;
     const int per = 2 * e->pairs_cap;
-    for (int z0 = 0; z0 < nplanes; z0 += per) {
+    // the second lane only when there are at least two batches
+    const bool two = e->lanes == 2 && nplanes > per;
+    Engine side_lane;
+    if (two) {
+        side_lane = *e;
+        side_lane.C = e->C2;
+        side_lane.est = e->est2;
+        if (!FMVD_CHECK(cudaEventRecord(e->ev_fork, s)) || !FMVD_CHECK(cudaStreamWaitEvent(e->side, e->ev_fork, 0)))
+            return false;
+    }
+    for (int z0 = 0, k = 0; z0 < nplanes; z0 += per, k++) {
         const int n = nplanes - z0 < per ? nplanes - z0 : per;
-        engine_batch(e, (const char *)data + z0 * plane * es, view_stride, (char *)out + z0 * plane * es, n,
-                     iterations, s, init ? init + (size_t)z0 * e->dims.H * e->dims.W : nullptr);
+        const bool on_side = two && (k & 1);
+        Engine *lane = on_side ? &side_lane : e;
+        const cudaStream_t ls = on_side ? e->side : s;
+        engine_batch(lane, (const char *)data + z0 * plane * es, view_stride, (char *)out + z0 * plane * es, n,
+                     iterations, ls, init ? init + (size_t)z0 * fplane : nullptr);
         if (est_out)
-            rl_split_estimate(e->dims, e->est, n, est_out + (size_t)z0 * e->dims.H * e->dims.W, s);
+            rl_split_estimate(e->dims, lane->est, n, est_out + (size_t)z0 * fplane, ls);
         if (!FMVD_CHECK(cudaGetLastError()))
             return false;
     }
+    if (two && (!FMVD_CHECK(cudaEventRecord(e->ev_join, e->side)) || !FMVD_CHECK(cudaStreamWaitEvent(s, e->ev_join, 0))))
+        return false;
     return true;
 }
 

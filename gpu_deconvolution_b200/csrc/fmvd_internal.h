@@ -36,16 +36,26 @@ struct Engine {
     float2 *twH, *twW;      // exp(-2 pi i n / N), block engine
     float2 *wtwH, *wtwW;    // warp engine twiddle tables
     int *status;            // device flag: a bulk-copy wait timed out
+    // Second lane: alternate batches run on a side stream with their own
+    // work planes, so one batch's passes fill the idle SMs of the other's
+    // last waves (lanes = 1: a single lane, no side stream).
+    int lanes;
+    float2 *C2, *est2;      // pairs_cap x H x W each (lanes = 2)
+    cudaStream_t side;
+    cudaEvent_t ev_fork, ev_join;
 };
 
 // Build an engine.  h_Kernel is normalised in place (reference semantics).
 // pairs_cap <= 0 selects the default batch size.  Returns null after
 // reporting an error.
 // col_warps: column-pass warps per block (2, 4 or 8; 0 = widest that fits).
+// lanes: 2 for device plans (engine_run alternates batches over two work
+// buffer sets and streams), 1 where the caller pipelines batches itself.
+// pairs_cap <= 0: the L2-sized default, split over the lanes.
 Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weights, float **h_Kernel, int kH,
-                      int kW, int psf_type, int nViews, int pairs_cap, int col_warps = 0);
+                      int kW, int psf_type, int nViews, int pairs_cap, int col_warps = 0, int lanes = 2);
 void engine_destroy(Engine *e);
-int default_pairs_cap(int H, int W);
+int default_pairs_cap(int H, int W, int lanes = 1);
 
 // Deconvolve nplanes planes resident on the device.  View v, plane z of the
 // input is at data + (v * view_stride + z * plane) samples; plane z of the

@@ -99,6 +99,7 @@ extern "C" int fmvd_b200_deconvolve_device_noalloc(fmvd_b200_plan *plan, const v
     run.status = reinterpret_cast<int *>(base);
     run.C = reinterpret_cast<float2 *>(base + kStatusBytes);
     run.est = run.C + (size_t)run.pairs_cap * points;
+    run.lanes = 1;  // one set of work planes: the shared array
 
     if (!FMVD_CHECK(cudaMemsetAsync(run.status, 0, sizeof(int), s)))
         return 1;

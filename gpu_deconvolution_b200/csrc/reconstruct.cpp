@@ -80,7 +80,7 @@ fmvd_b200_reconstructor *fmvd_b200_reconstructor_create(fmvd_b200_plan *plan, in
     r->es = r->bits == 16 ? 2 : 1;
     r->pitch = fmvd::source_pitch(r->bits, w);
     const int batch = 2 * plan->eng->pairs_cap;
-    int chunk = chunk_planes > 0 ? chunk_planes : 4 * batch;
+    int chunk = chunk_planes > 0 ? chunk_planes : 8 * batch;
     if (chunk > td)
         chunk = td;
     r->chunk = chunk;

@@ -294,9 +294,8 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
     const int g = lane / T, t = lane % T;
     const int gi = warp * G + g;
     float *gbase = smem + (size_t)gi * a.group_floats;
-    float *bre = gbase;
-    float *bim = bre + W;
-    char *pf = reinterpret_cast<char *>(gbase + WF::group_floats);  // prefetch area, 16-byte aligned
+    float2 *tbuf = reinterpret_cast<float2 *>(gbase);                // padded transpose buffer
+    char *pf = reinterpret_cast<char *>(gbase + WF::padded_floats);  // prefetch area, 16-byte aligned
     const int H = a.d.H;
     const int yr = blockIdx.x * (kRowWarps * G) + warp * G + g;
     const bool valid = yr < H;
@@ -360,7 +359,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
                 v[m] = make_float2(x.x, -x.y);
             }
         }
-        WF::template run<-1>(v, a.tw, bre, bim, t);
+        WF::template run_padded<-1>(v, a.tw, tbuf, t);
         if (pass == 1)
             break;
 #pragma unroll
@@ -811,7 +810,7 @@ static void launch_row(const RowArgs &a0, cudaStream_t s)
             pf = W * sizeof(float2) + (a.bulk_weights ? a.d.dataW * sizeof(float) : 0);
         else if (MODE == ROW_DIVIDE && a.bulk_data)
             pf = 2 * ((a.d.dataW * es + 15) & ~(size_t)15);
-        a.group_floats = WF::group_floats + (int)(pf / sizeof(float));
+        a.group_floats = WF::padded_floats + (int)(pf / sizeof(float));
         const size_t smem = sizeof(float) * kRowWarps * G * (size_t)a.group_floats;
         auto kern = row_pass_w<W, MODE>;
         static unsigned mask = 0;

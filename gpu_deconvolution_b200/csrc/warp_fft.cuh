@@ -158,34 +158,86 @@ struct WarpFft {
         run_addr<DIR>(v, tw, bre, bim, t, StridedAddr<STRIDE>());
     }
 
+    // Step 2: v[k1] *= w_N^(t k1), k1 < E (table entries times a recurrence).
+    template <int DIR>
+    static __device__ __forceinline__ void twiddle(float2 *v, const float2 *__restrict__ tw, int t)
+    {
+        const float2 w1 = __ldg(tw + J * T + t);
+        float2 wp[R8];
+        wp[0] = make_float2(1.f, 0.f);
+        if (R8 > 1)
+            wp[1] = w1;
+#pragma unroll
+        for (int b = 2; b < R8; b++)
+            wp[b] = cmul(wp[b - 1], w1);
+#pragma unroll
+        for (int j = 0; j < J; j++) {
+            const float2 wj = j == 0 ? make_float2(1.f, 0.f) : __ldg(tw + j * T + t);
+#pragma unroll
+            for (int b = 0; b < R8; b++) {
+                const int k1 = j * R8 + b;
+                if (k1 == 0)
+                    continue;
+                const float2 w = j == 0 ? wp[b] : (b == 0 ? wj : cmul(wj, wp[b]));
+                v[k1] = ctw<DIR>(v[k1], w);
+            }
+        }
+    }
+
+    // Step 4 output order: X[t + T s + E k2] is in v[s * T + k2]; move it to v[s + S k2].
+    static __device__ __forceinline__ void reorder(float2 *v)
+    {
+        if constexpr (S > 1) {
+            float2 o[E];
+#pragma unroll
+            for (int s = 0; s < S; s++)
+#pragma unroll
+                for (int k2 = 0; k2 < T; k2++)
+                    o[s + S * k2] = v[s * T + k2];
+#pragma unroll
+            for (int m = 0; m < E; m++)
+                v[m] = o[m];
+        }
+    }
+
+    // Complex (float2) elements of a group's padded transpose buffer: row k1
+    // of T + 1 entries, so that the writes (lane t, fixed k1) and the reads
+    // (lane t, row t + T s) are both free of bank conflicts with 64-bit
+    // accesses at compile-time offsets.
+    static constexpr int padded_f2 = E * (T + 1);
+    static constexpr int padded_floats = ((2 * padded_f2 + 3) / 4) * 4;  // 16-byte multiple
+
+    // The transform with the transpose through the padded float2 buffer buf.
+    template <int DIR>
+    static __device__ __forceinline__ void run_padded(float2 *v, const float2 *__restrict__ tw, float2 *buf, int t)
+    {
+        Dft<E, DIR>::run(v);
+        twiddle<DIR>(v, tw, t);
+        float2 *wr = buf + t;
+#pragma unroll
+        for (int k1 = 0; k1 < E; k1++)
+            wr[k1 * (T + 1)] = v[k1];
+        __syncwarp();
+        const float2 *rd = buf + t * (T + 1);
+#pragma unroll
+        for (int s = 0; s < S; s++)
+#pragma unroll
+            for (int j = 0; j < T; j++)
+                v[s * T + j] = rd[s * T * (T + 1) + j];
+        __syncwarp();
+#pragma unroll
+        for (int s = 0; s < S; s++)
+            Dft<T, DIR>::run(v + s * T);
+        reorder(v);
+    }
+
     // Same, with the transpose buffer element p at bre[addr(p)] / bim[addr(p)].
     template <int DIR, typename Addr>
     static __device__ __forceinline__ void run_addr(float2 *v, const float2 *__restrict__ tw, float *bre, float *bim,
                                                     int t, const Addr &addr)
     {
         Dft<E, DIR>::run(v);
-        {
-            const float2 w1 = __ldg(tw + J * T + t);
-            float2 wp[R8];
-            wp[0] = make_float2(1.f, 0.f);
-            if (R8 > 1)
-                wp[1] = w1;
-#pragma unroll
-            for (int b = 2; b < R8; b++)
-                wp[b] = cmul(wp[b - 1], w1);
-#pragma unroll
-            for (int j = 0; j < J; j++) {
-                const float2 wj = j == 0 ? make_float2(1.f, 0.f) : __ldg(tw + j * T + t);
-#pragma unroll
-                for (int b = 0; b < R8; b++) {
-                    const int k1 = j * R8 + b;
-                    if (k1 == 0)
-                        continue;
-                    const float2 w = j == 0 ? wp[b] : (b == 0 ? wj : cmul(wj, wp[b]));
-                    v[k1] = ctw<DIR>(v[k1], w);
-                }
-            }
-        }
+        twiddle<DIR>(v, tw, t);
 #pragma unroll
         for (int k1 = 0; k1 < E; k1++) {
             const int p = addr(tpos(k1, t));
@@ -206,18 +258,7 @@ struct WarpFft {
 #pragma unroll
         for (int s = 0; s < S; s++)
             Dft<T, DIR>::run(v + s * T);
-        // X[t + T s + E k2] is in v[s * T + k2]; reorder to v[s + S k2]
-        if constexpr (S > 1) {
-            float2 o[E];
-#pragma unroll
-            for (int s = 0; s < S; s++)
-#pragma unroll
-                for (int k2 = 0; k2 < T; k2++)
-                    o[s + S * k2] = v[s * T + k2];
-#pragma unroll
-            for (int m = 0; m < E; m++)
-                v[m] = o[m];
-        }
+        reorder(v);
     }
 };
 

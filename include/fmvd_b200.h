@@ -111,7 +111,7 @@ struct fmvd_plan_cuda_8 *fmvd_b200_initialize_cuda_8(int dataH, int dataW, float
  * frame to the host and streams it back plane by plane).  A reconstructor
  * holds the device buffers for one geometry: V source volumes of d planes of
  * h x w samples, a td-plane frame of th x tw (the plan's data plane), work in
- * chunks of chunk_planes target planes (0 = four plan batches). */
+ * chunks of chunk_planes target planes (0 = eight plan batches). */
 typedef struct fmvd_b200_reconstructor fmvd_b200_reconstructor;
 fmvd_b200_reconstructor *fmvd_b200_reconstructor_create(fmvd_b200_plan *plan, int views, int w, int h, int d,
                                                         int tw, int th, int td, int chunk_planes);
