@@ -225,7 +225,7 @@ Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weig
     e->kH = kH;
     e->kW = kW;
     e->device = dev;
-    e->lanes = lanes > 1 ? 2 : 1;
+    e->lanes = lanes < 1 ? 1 : (lanes > kMaxLanes ? kMaxLanes : lanes);
     e->pairs_cap = pairs_cap > 0 ? pairs_cap : default_pairs_cap(H, W, e->lanes);
     e->spec_elems = rl_spectrum_elems(H, W);
 
@@ -246,12 +246,13 @@ Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weig
               FMVD_CHECK(cudaMalloc(&e->twH, sizeof(float2) * H)) && FMVD_CHECK(cudaMalloc(&e->twW, sizeof(float2) * W)) &&
               FMVD_CHECK(cudaMalloc(&e->wtwH, sizeof(float2) * H)) && FMVD_CHECK(cudaMalloc(&e->wtwW, sizeof(float2) * W)) &&
               FMVD_CHECK(cudaMalloc(&e->status, sizeof(int))) && FMVD_CHECK(cudaMemset(e->status, 0, sizeof(int)));
-    if (ok && e->lanes == 2)
-        ok = FMVD_CHECK(cudaMalloc(&e->C2, sizeof(float2) * (size_t)H * W * e->pairs_cap)) &&
-             FMVD_CHECK(cudaMalloc(&e->est2, sizeof(float2) * (size_t)H * W * e->pairs_cap)) &&
-             FMVD_CHECK(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking)) &&
-             FMVD_CHECK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming)) &&
-             FMVD_CHECK(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
+    if (ok && e->lanes > 1)
+        ok = FMVD_CHECK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+    for (int l = 0; ok && l + 1 < e->lanes; l++)
+        ok = FMVD_CHECK(cudaMalloc(&e->laneC[l], sizeof(float2) * (size_t)H * W * e->pairs_cap)) &&
+             FMVD_CHECK(cudaMalloc(&e->laneEst[l], sizeof(float2) * (size_t)H * W * e->pairs_cap)) &&
+             FMVD_CHECK(cudaStreamCreateWithFlags(&e->side[l], cudaStreamNonBlocking)) &&
+             FMVD_CHECK(cudaEventCreateWithFlags(&e->ev_join[l], cudaEventDisableTiming));
     if (!ok) {
         engine_destroy(e);
         return nullptr;
@@ -329,14 +330,16 @@ void engine_destroy(Engine *e)
     cudaFree(e->wtwH);
     cudaFree(e->wtwW);
     cudaFree(e->status);
-    cudaFree(e->C2);
-    cudaFree(e->est2);
-    if (e->side)
-        cudaStreamDestroy(e->side);
+    for (int l = 0; l + 1 < kMaxLanes; l++) {
+        cudaFree(e->laneC[l]);
+        cudaFree(e->laneEst[l]);
+        if (e->side[l])
+            cudaStreamDestroy(e->side[l]);
+        if (e->ev_join[l])
+            cudaEventDestroy(e->ev_join[l]);
+    }
     if (e->ev_fork)
         cudaEventDestroy(e->ev_fork);
-    if (e->ev_join)
-        cudaEventDestroy(e->ev_join);
     delete e;
 }
 
@@ -399,21 +402,27 @@ bool engine_run(Engine *e, const void *data, size_t view_stride, void *out, int 
     const size_t fplane = (size_t)e->dims.H * e->dims.W;
     const size_t es = e->dims.bits == 16 ? 2 : 1;
     const int per = 2 * e->pairs_cap;
-    // the second lane only when there are at least two batches
-    const bool two = e->lanes == 2 && nplanes > per;
-    Engine side_lane;
-    if (two) {
-        side_lane = *e;
-        side_lane.C = e->C2;
-        side_lane.est = e->est2;
-        if (!FMVD_CHECK(cudaEventRecord(e->ev_fork, s)) || !FMVD_CHECK(cudaStreamWaitEvent(e->side, e->ev_fork, 0)))
+    // more lanes only when there are several batches
+    const int nbatches = (nplanes + per - 1) / per;
+    const int used = e->lanes < nbatches ? e->lanes : nbatches;
+    Engine lane_eng[kMaxLanes];
+    cudaStream_t lane_s[kMaxLanes];
+    lane_eng[0] = *e;
+    lane_s[0] = s;
+    if (used > 1 && !FMVD_CHECK(cudaEventRecord(e->ev_fork, s)))
+        return false;
+    for (int l = 1; l < used; l++) {
+        lane_eng[l] = *e;
+        lane_eng[l].C = e->laneC[l - 1];
+        lane_eng[l].est = e->laneEst[l - 1];
+        lane_s[l] = e->side[l - 1];
+        if (!FMVD_CHECK(cudaStreamWaitEvent(lane_s[l], e->ev_fork, 0)))
             return false;
     }
     for (int z0 = 0, k = 0; z0 < nplanes; z0 += per, k++) {
         const int n = nplanes - z0 < per ? nplanes - z0 : per;
-        const bool on_side = two && (k & 1);
-        Engine *lane = on_side ? &side_lane : e;
-        const cudaStream_t ls = on_side ? e->side : s;
+        Engine *lane = &lane_eng[k % used];
+        const cudaStream_t ls = lane_s[k % used];
         engine_batch(lane, (const char *)data + z0 * plane * es, view_stride, (char *)out + z0 * plane * es, n,
                      iterations, ls, init ? init + (size_t)z0 * fplane : nullptr);
         if (est_out)
@@ -421,8 +430,10 @@ bool engine_run(Engine *e, const void *data, size_t view_stride, void *out, int 
         if (!FMVD_CHECK(cudaGetLastError()))
             return false;
     }
-    if (two && (!FMVD_CHECK(cudaEventRecord(e->ev_join, e->side)) || !FMVD_CHECK(cudaStreamWaitEvent(s, e->ev_join, 0))))
-        return false;
+    for (int l = 1; l < used; l++)
+        if (!FMVD_CHECK(cudaEventRecord(e->ev_join[l - 1], lane_s[l])) ||
+            !FMVD_CHECK(cudaStreamWaitEvent(s, e->ev_join[l - 1], 0)))
+            return false;
     return true;
 }
 

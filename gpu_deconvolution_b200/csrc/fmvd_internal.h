@@ -40,20 +40,28 @@ struct Engine {
     // work planes, so one batch's passes fill the idle SMs of the other's
     // last waves (lanes = 1: a single lane, no side stream).
     int lanes;
-    float2 *C2, *est2;      // pairs_cap x H x W each (lanes = 2)
-    cudaStream_t side;
-    cudaEvent_t ev_fork, ev_join;
+    float2 *laneC[3], *laneEst[3];   // lanes 1.. : pairs_cap x H x W each
+    cudaStream_t side[3];
+    cudaEvent_t ev_fork, ev_join[3];
 };
+
+// Lanes of a device plan (batches in flight on separate streams).
+#ifndef FMVD_ENGINE_LANES
+#define FMVD_ENGINE_LANES 2
+#endif
+constexpr int kMaxLanes = 4;
 
 // Build an engine.  h_Kernel is normalised in place (reference semantics).
 // pairs_cap <= 0 selects the default batch size.  Returns null after
 // reporting an error.
 // col_warps: column-pass warps per block (2, 4 or 8; 0 = widest that fits).
-// lanes: 2 for device plans (engine_run alternates batches over two work
-// buffer sets and streams), 1 where the caller pipelines batches itself.
-// pairs_cap <= 0: the L2-sized default, split over the lanes.
+// lanes: FMVD_ENGINE_LANES for device plans (engine_run deals batches
+// round-robin over that many work buffer sets and streams), 1 where the
+// caller pipelines batches itself.  pairs_cap <= 0: the L2-sized default,
+// split over the lanes.
 Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weights, float **h_Kernel, int kH,
-                      int kW, int psf_type, int nViews, int pairs_cap, int col_warps = 0, int lanes = 2);
+                      int kW, int psf_type, int nViews, int pairs_cap, int col_warps = 0,
+                      int lanes = FMVD_ENGINE_LANES);
 void engine_destroy(Engine *e);
 int default_pairs_cap(int H, int W, int lanes = 1);
 
