@@ -235,8 +235,15 @@ __device__ __forceinline__ void pointwise(const RowArgs &a, int p, int y, int x,
 }
 
 // Row pass for W > 1024: F rows per block through the shared-memory Stockham engine.
+// Blocks per SM the register allocation of the block-engine passes must allow.
+#ifndef FMVD_BLOCK_ROW_MIN_BLOCKS
+#define FMVD_BLOCK_ROW_MIN_BLOCKS 1
+#endif
+#ifndef FMVD_BLOCK_COL_MIN_BLOCKS
+#define FMVD_BLOCK_COL_MIN_BLOCKS 1
+#endif
 template <int W, int F, int MODE>
-__global__ void __launch_bounds__(Cfg<W, F>::NT) row_pass(const RowArgs a)
+__global__ void __launch_bounds__(Cfg<W, F>::NT, FMVD_BLOCK_ROW_MIN_BLOCKS) row_pass(const RowArgs a)
 {
     extern __shared__ float smem[];
     float *sre = smem;
@@ -253,11 +260,21 @@ __global__ void __launch_bounds__(Cfg<W, F>::NT) row_pass(const RowArgs a)
         __syncthreads();
         fft<W, F, NT, +1, false>(sre, sim, v, a.tw);
     }
+    {
+        // the element-wise state of this thread's first row, built once (a
+        // thread's slots usually all lie in one row)
+        int f0, x0;
+        EG::pos(0, f0, x0);
+        const RowWork<MODE> w0(a, p, y0 + f0);
 #pragma unroll
-    for (int e = 0; e < EG::E; e++) {
-        int f, x;
-        EG::pos(e, f, x);
-        pointwise<MODE>(a, p, y0 + f, x, v[e]);
+        for (int e = 0; e < EG::E; e++) {
+            int f, x;
+            EG::pos(e, f, x);
+            if (f == f0)
+                w0.apply(x, v[e]);
+            else
+                pointwise<MODE>(a, p, y0 + f, x, v[e]);
+        }
     }
     if (MODE == ROW_UPDATE && a.last)
         return;
@@ -410,7 +427,7 @@ struct ColArgs {
 };
 
 template <int H, int F>
-__global__ void __launch_bounds__(Cfg<H, F>::NT) col_pass(const ColArgs a)
+__global__ void __launch_bounds__(Cfg<H, F>::NT, FMVD_BLOCK_COL_MIN_BLOCKS) col_pass(const ColArgs a)
 {
     extern __shared__ float smem[];
     float *sre = smem;
