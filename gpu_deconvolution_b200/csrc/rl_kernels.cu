@@ -242,18 +242,65 @@ __device__ __forceinline__ void pointwise(const RowArgs &a, int p, int y, int x,
 #ifndef FMVD_BLOCK_COL_MIN_BLOCKS
 #define FMVD_BLOCK_COL_MIN_BLOCKS 1
 #endif
+// Shared-memory prefetch of the element-wise operand rows of a block-engine
+// row pass: bytes after the transform arrays.
+template <int W, int F>
+struct BlockRowPrefetch {
+    static constexpr size_t offset = (Cfg<W, F>::smem + 15) & ~(size_t)15;
+    static __host__ __device__ size_t row_bytes(size_t b) { return (b + 15) & ~(size_t)15; }
+};
+
 template <int W, int F, int MODE>
 __global__ void __launch_bounds__(Cfg<W, F>::NT, FMVD_BLOCK_ROW_MIN_BLOCKS) row_pass(const RowArgs a)
 {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) float smem[];
+    __shared__ __align__(8) uint64_t pbar;
     float *sre = smem;
     float *sim = smem + SmemLayout<W>::floats(F);
     constexpr int NT = Cfg<W, F>::NT;
     using EG = Edge<W, F, NT>;
+    using PF = BlockRowPrefetch<W, F>;
     const int p = blockIdx.y;
     const int y0 = blockIdx.x * F;
     float2 *C = a.b.C + (size_t)p * a.d.H * W + (size_t)y0 * W;
     float2 v[EG::E];
+
+    // The estimate and weight rows (update) or the data rows (divide) of the
+    // block's F rows arrive by bulk copy while the inverse transform runs.
+    char *pf = reinterpret_cast<char *>(smem) + PF::offset;
+    const int es = a.d.bits == 16 ? 2 : 1;
+    const bool has1 = 2 * p + 1 < a.b.nplanes;
+    const size_t wrb = PF::row_bytes((size_t)a.d.dataW * sizeof(float));
+    const size_t drb = PF::row_bytes((size_t)a.d.dataW * es);
+    const bool prefetch = (MODE == ROW_UPDATE) || (MODE == ROW_DIVIDE && a.bulk_data);
+    if (prefetch && threadIdx.x == 0) {
+        mbar_init(&pbar, 1);
+        mbar_fence_init();
+        if (MODE == ROW_UPDATE) {
+            const uint32_t eb = F * W * sizeof(float2);
+            const uint32_t wb = a.bulk_weights ? F * (uint32_t)a.d.dataW * sizeof(float) : 0;
+            mbar_arrive_expect_tx(&pbar, eb + wb);
+            bulk_load(pf, a.b.est + ((size_t)p * a.d.H + y0) * W, eb, &pbar);
+            if (a.bulk_weights)
+                for (int f = 0; f < F; f++)
+                    bulk_load(pf + eb + f * wrb,
+                              a.b.weights + (size_t)a.view * a.d.dataH * a.d.dataW +
+                                  (size_t)clamp_src(y0 + f, a.d.dataH, a.d.byW) * a.d.dataW,
+                              a.d.dataW * sizeof(float), &pbar);
+        } else {
+            const uint32_t rb = a.d.dataW * es;
+            mbar_arrive_expect_tx(&pbar, F * rb * (has1 ? 2 : 1));
+            for (int f = 0; f < F; f++) {
+                const size_t base = (size_t)a.view * a.b.view_stride +
+                                    (size_t)clamp_src(y0 + f, a.d.dataH, a.d.byD) * a.d.dataW;
+                bulk_load(pf + (2 * f) * drb, (const char *)a.b.data + (base + (size_t)(2 * p) * a.b.plane_stride) * es,
+                          rb, &pbar);
+                if (has1)
+                    bulk_load(pf + (2 * f + 1) * drb,
+                              (const char *)a.b.data + (base + (size_t)(2 * p + 1) * a.b.plane_stride) * es, rb, &pbar);
+            }
+        }
+    }
 
     if (MODE != ROW_INIT) {
         load_rows<W, F>(C, sre, sim);
@@ -265,7 +312,26 @@ __global__ void __launch_bounds__(Cfg<W, F>::NT, FMVD_BLOCK_ROW_MIN_BLOCKS) row_
         // thread's slots usually all lie in one row)
         int f0, x0;
         EG::pos(0, f0, x0);
-        const RowWork<MODE> w0(a, p, y0 + f0);
+        RowWork<MODE> w0(a, p, y0 + f0);
+        if (prefetch) {
+            if (!mbar_wait(&pbar, 0)) {
+                // the copies did not land in time: flag it, wait once more so
+                // none is left in flight, and read from global memory
+                if (threadIdx.x == 0)
+                    atomicExch(a.b.status, 1);
+                mbar_wait(&pbar, 0);
+            } else if (MODE == ROW_UPDATE) {
+                w0.est_s = reinterpret_cast<const float2 *>(pf) + (size_t)f0 * W;
+                if (a.bulk_weights) {
+                    w0.wrow = reinterpret_cast<const float *>(pf + F * W * sizeof(float2) + f0 * wrb);
+                    w0.w_s = true;
+                }
+            } else {
+                w0.src0 = pf + (2 * f0) * drb;
+                w0.src1 = has1 ? pf + (2 * f0 + 1) * drb : w0.src0;
+                w0.src_s = true;
+            }
+        }
 #pragma unroll
         for (int e = 0; e < EG::E; e++) {
             int f, x;
@@ -836,12 +902,24 @@ static void launch_row(const RowArgs &a0, cudaStream_t s)
         kern<<<grid, kRowWarps * 32, smem, s>>>(a);
     } else {
         constexpr int F = row_f(W);
-        using C = Cfg<W, F>;
+        using PF = BlockRowPrefetch<W, F>;
+        RowArgs a = a0;
+        const size_t es = a.d.bits == 16 ? 2 : 1;
+        a.bulk_data = aligned16(a.b.data, a.d.dataW * es) && (a.b.view_stride * es) % 16 == 0 &&
+                      (a.b.plane_stride * es) % 16 == 0;
+        a.bulk_weights = aligned16(a.b.weights, a.d.dataW * sizeof(float)) &&
+                         ((size_t)a.d.dataH * a.d.dataW * sizeof(float)) % 16 == 0;
+        size_t pf = 0;
+        if (MODE == ROW_UPDATE)
+            pf = F * W * sizeof(float2) + (a.bulk_weights ? F * PF::row_bytes(a.d.dataW * sizeof(float)) : 0);
+        else if (MODE == ROW_DIVIDE && a.bulk_data)
+            pf = 2 * F * PF::row_bytes(a.d.dataW * es);
+        const size_t smem = PF::offset + pf;
         auto kern = row_pass<W, F, MODE>;
         static unsigned mask = 0;
-        configure_smem(kern, C::smem, mask);
-        dim3 grid(a0.d.H / F, a0.b.npairs);
-        kern<<<grid, C::NT, C::smem, s>>>(a0);
+        configure_smem(kern, 200 * 1024, mask);
+        dim3 grid(a.d.H / F, a.b.npairs);
+        kern<<<grid, Cfg<W, F>::NT, smem, s>>>(a);
     }
     g_launches++;
 }
