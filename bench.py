@@ -62,7 +62,7 @@ def parse():
     p.add_argument("--small", action="store_true", help="small volume for profiler captures")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--workload", default="transform_rl", choices=["transform_rl", "warmstart"],
+    p.add_argument("--workload", default="transform_rl", choices=["transform_rl", "warmstart", "batched"],
                    help="warmstart: learned warm start vs plain RL-50 (time to the RL-50 result)")
     p.add_argument("--train-planes", type=int, default=4000)
     p.add_argument("--epochs", type=int, default=12)
@@ -540,12 +540,65 @@ def run_warmstart(args):
     net.destroy()
 
 
+def run_batched(args):
+    """Batched uneven plain RL: 32 independent volumes (planes 128..1024
+    square, depths 16..256, 2-6 views, kernels 9..41, 25 iterations) run by
+    one CUDA graph launch (fmvd_b200_batch_*), against the same volumes run
+    one after another.  (Per-volume errors against the FP64 oracle are
+    checked by tests/test_batch_tune.py.)"""
+    import torch
+    from gpu_deconvolution_b200 import api
+    from gpu_deconvolution_b200 import synth as S
+    specs = S.batched_specs(0, 32)
+    plans, views, outs = [], [], []
+    for sp in specs:
+        w = [np.ones((sp["H"], sp["W"]), np.float32)] * sp["V"]
+        plans.append(api.DevicePlan(sp["H"], sp["W"], w, S.spec_psfs(sp), 0))
+        views.append(S.views_torch(sp))
+        outs.append(torch.zeros((sp["D"], sp["H"], sp["W"]), dtype=torch.int16, device="cuda"))
+    torch.cuda.synchronize()
+    its = [sp["iterations"] for sp in specs]
+    voxel_iters = sum(sp["D"] * sp["H"] * sp["W"] * sp["iterations"] for sp in specs)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    by_branches = {}
+    for nb in (1, 2, 4, 8):
+        batch = api.Batch(plans, views, outs, its, max_branches=nb)
+        batch.run()
+        torch.cuda.synchronize()
+        e0.record()
+        batch.run()
+        e1.record()
+        torch.cuda.synchronize()
+        by_branches[nb] = e0.elapsed_time(e1)
+        batch.destroy()
+    best = min(by_branches, key=by_branches.get)
+    t_graph = by_branches[best] / 1e3
+    e0.record()
+    for p, v, o, it in zip(plans, views, outs, its):
+        p.run(v, o, it)
+    e1.record()
+    torch.cuda.synchronize()
+    t_seq = e0.elapsed_time(e1) / 1e3
+    for p in plans:
+        p.destroy()
+    print(json.dumps({
+        "metric": "RL voxel-iter/s, 32 uneven volumes in one graph launch", "unit": UNIT,
+        "value": voxel_iters / t_graph, "ms": t_graph * 1e3, "branches": best,
+        "ms_by_branches": by_branches, "sequential_ms": t_seq * 1e3,
+        "graph_speedup": t_seq / t_graph, "volumes": len(specs), "voxel_iters": voxel_iters,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batched uneven plain RL (32 volumes, planes 128..1024, depths 16..256, 2-6 views, "
+                               "kernels 9..41, 25 iterations)"}}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "warmstart":
         run_warmstart(args)
+    elif args.workload == "batched":
+        run_batched(args)
     else:
         run_b200(args)
 

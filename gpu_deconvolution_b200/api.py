@@ -321,7 +321,7 @@ class Batch:
     deconvolved by one CUDA graph launch (fmvd_b200_batch_*).  The plans and
     tensors must outlive the batch."""
 
-    def __init__(self, plans, views, outs, iterations, max_branches=8):
+    def __init__(self, plans, views, outs, iterations, max_branches=1):
         self.lib = native.load()
         n = len(plans)
         its = iterations if isinstance(iterations, (list, tuple)) else [iterations] * n

@@ -3,14 +3,17 @@
 //
 // Each volume keeps its own plan (spectra, weights, work planes).  At
 // creation the launch sequences of all volumes are captured once into one
-// graph whose branches run concurrently: small planes fill only part of the
-// GPU, so volumes on different branches overlap, and the host issues a single
-// graph launch per run instead of a few thousand kernel launches.  Volumes
-// that share a plan share its work planes, so they go to the same branch and
-// run in order.
+// graph; the host issues a single graph launch per run instead of thousands
+// of kernel launches.  The graph may have several concurrent branches
+// (balanced by estimated work); volumes that share a plan share its work
+// planes, so they go to the same branch and run in order.  Each plan already
+// runs two batch lanes and keeps its batches resident in L2, so concurrent
+// branches evict each other: on the 32-volume workload one branch measured
+// fastest, and it is the default.
 #include "fmvd_b200.h"
 #include "fmvd_internal.h"
 
+#include <algorithm>
 #include <map>
 #include <vector>
 
@@ -58,20 +61,32 @@ fmvd_b200_batch *fmvd_b200_batch_create(int count, fmvd_b200_plan *const *plans,
             return nullptr;
         }
     if (max_branches < 1)
-        max_branches = 8;
+        max_branches = 1;
 
-    // branch of each volume: one per distinct plan, round robin over the
-    // allowed number of branches
-    std::map<const fmvd_b200_plan *, int> branch_of_plan;
-    std::vector<int> branch(count);
-    int next = 0;
-    for (int i = 0; i < count; i++) {
-        auto it = branch_of_plan.find(plans[i]);
-        if (it == branch_of_plan.end())
-            it = branch_of_plan.emplace(plans[i], next++ % max_branches).first;
-        branch[i] = it->second;
+    // Branch of each volume: volumes sharing a plan stay together; groups go,
+    // largest estimated work first, to the branch with the least work so far
+    // (work ~ planes x padded plane x views x iterations).
+    std::map<const fmvd_b200_plan *, std::vector<int>> groups;
+    for (int i = 0; i < count; i++)
+        groups[plans[i]].push_back(i);
+    std::vector<std::pair<double, const fmvd_b200_plan *>> order;
+    for (auto &g : groups) {
+        const fmvd::RlDims &d = g.first->eng->dims;
+        double w = 0;
+        for (int i : g.second)
+            w += (double)nplanes[i] * d.H * d.W * d.V * (iterations[i] > 0 ? iterations[i] : 1);
+        order.push_back({w, g.first});
     }
-    const int nb = next < max_branches ? next : max_branches;
+    std::sort(order.begin(), order.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+    const int nb = (int)order.size() < max_branches ? (int)order.size() : max_branches;
+    std::vector<double> load(nb, 0.0);
+    std::vector<int> branch(count);
+    for (auto &o : order) {
+        const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[k] += o.first;
+        for (int i : groups[o.second])
+            branch[i] = k;
+    }
 
     fmvd_b200_batch *b = new fmvd_b200_batch();
     b->branches = nb;

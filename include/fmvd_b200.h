@@ -82,8 +82,11 @@ int fmvd_b200_deconvolve_device_noalloc(fmvd_b200_plan *plan, const void *d_view
 /* Captures, once, the deconvolution of 'count' device-resident volumes
  * (volume i: plans[i], d_views[i] with view_strides[i], d_outs[i],
  * nplanes[i] planes, iterations[i]) into one CUDA graph with up to
- * max_branches concurrent branches (0 = 8).  Volumes that share a plan run
- * in order on one branch.  Buffers must stay valid while the batch exists. */
+ * max_branches concurrent branches (0 = 1), balanced by estimated work.
+ * Volumes that share a plan run in order on one branch.  Each branch keeps
+ * its current batch resident in L2, so more branches only pay for small
+ * planes.
+ * Buffers must stay valid while the batch exists. */
 typedef struct fmvd_b200_batch fmvd_b200_batch;
 fmvd_b200_batch *fmvd_b200_batch_create(int count, fmvd_b200_plan *const *plans, const void *const *d_views,
                                         const size_t *view_strides, void *const *d_outs, const int *nplanes,

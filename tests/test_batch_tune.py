@@ -153,3 +153,37 @@ def test_tuned_plan_is_bit_identical(tmp_path):
     finally:
         tuned.destroy()
         default.destroy()
+
+
+@pytest.mark.gpu
+def test_batched_workload_volumes_against_oracle():
+    """Per-volume error of the batched workload (32 volumes, seed 0) against
+    the FP64 oracle, on the middle plane of every volume whose padded plane is
+    at most 512 x 512 (the oracle's cost bounds the rest): within the RL
+    parity tolerance of 1e-4 relative L2."""
+    import torch
+    from gpu_deconvolution_b200 import api
+    from oracle import fmvd_oracle as O
+    checked = 0
+    for sp in synth.batched_specs(0, 32):
+        if O.snap_transform_size(sp["H"] + sp["k"] - 1) > 512:
+            continue
+        psfs = synth.spec_psfs(sp)
+        w = [np.ones((sp["H"], sp["W"]), np.float32)] * sp["V"]
+        views = synth.views_torch(sp)
+        z = sp["D"] // 2
+        one = views[:, z:z + 1].contiguous()
+        plan = api.DevicePlan(sp["H"], sp["W"], w, [p.copy() for p in psfs], 0)
+        try:
+            est = torch.zeros((1, plan.fftH, plan.fftW), dtype=torch.float32, device="cuda")
+            out = torch.zeros((1, sp["H"], sp["W"]), dtype=torch.int16, device="cuda")
+            plan.run(one, out, sp["iterations"], estimate=est)
+            torch.cuda.synchronize()
+        finally:
+            plan.destroy()
+        vv = one[:, 0].cpu().numpy().view(np.uint16)
+        ref = O.Plan(sp["H"], sp["W"], w, psfs, 0).deconvolve_plane([vv[v] for v in range(sp["V"])],
+                                                                    sp["iterations"])
+        assert rel_l2(est[0].cpu().numpy(), ref) < 1e-4, sp["index"]
+        checked += 1
+    assert checked >= 5
