@@ -319,7 +319,7 @@ def run_b200(args):
 
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(args, vols, mats, psfs, weights, src, frame)
+        e2e = run_e2e(args, vols, mats, psfs, weights, src, frame, world)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         frames = frame_dev[:, :min(96, td)].cpu().numpy().view(np.uint16)
@@ -358,7 +358,7 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
-def run_e2e(args, vols, mats, psfs, weights, src, frame):
+def run_e2e(args, vols, mats, psfs, weights, src, frame, world=1):
     """The same step end to end through the C ABI with host buffers: pinned
     source volumes in, the result in host memory out
     (fmvd_b200_reconstruct_host: sources uploaded once, resampling and RL in
@@ -376,10 +376,11 @@ def run_e2e(args, vols, mats, psfs, weights, src, frame):
     try:
         rec.run(pinned, mats, ITERATIONS, out)
         n = max(1, min(args.steps, 3))
+        barrier(world)
         t0 = time.perf_counter()
         for _ in range(n):
             rec.run(pinned, mats, ITERATIONS, out)
-        dt = (time.perf_counter() - t0) / n
+        dt = barrier_max((time.perf_counter() - t0) / n, world)  # slowest rank
     finally:
         rec.destroy()
         plan.destroy()
@@ -392,11 +393,11 @@ def run_e2e(args, vols, mats, psfs, weights, src, frame):
     ref_api_out = api.deconvolve(frames, weights, [p.copy() for p in psfs], 0, ITERATIONS, nstreams=3)
     dt_ref_api = time.perf_counter() - t0
     assert ref_api_out.shape[0] == td
-    return {"value": td * th * tw * ITERATIONS / dt, "unit": UNIT, "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h, "ms_per_step": dt * 1e3,
+    return {"value": td * th * tw * ITERATIONS * world / dt, "unit": UNIT, "h2d_bytes_per_step": h2d * world,
+            "d2h_bytes_per_step": d2h * world, "ms_per_step": dt * 1e3,
             "api": "fmvd_b200_reconstruct_host (pinned sources in, result to host memory)",
             "reference_style_api": {
-                "value": td * th * tw * ITERATIONS / dt_ref_api, "ms_per_step": dt_ref_api * 1e3,
+                "value": td * th * tw * ITERATIONS / dt_ref_api, "ms_per_step": dt_ref_api * 1e3, "gpus": 1,
                 "api": "fmvd_b200_transform_host x4 + fmvd_initialize/deconvolve_planes/destroy_cuda_16 "
                        "(frame through host memory, per-plane callbacks)",
                 "h2d_bytes_per_step": h2d + V * td * th * tw * 2, "d2h_bytes_per_step": V * td * th * tw * 2 + d2h}}
