@@ -6,7 +6,7 @@ mean to an estimate of that plane.  It is trained only on pairs the method
 itself produces: views and the plain RL-N result from the reference's
 initialisation.  At inference the network's estimate, padded like the views,
 starts RL (``DevicePlan.run(init=...)``) for k iterations instead of N;
-plain RL-N stays the judge of its error and the fallback:
+plain RL-N remains the measure of its error and the fallback:
 
 * ``WarmStartNet``      the network (train_step, forward, parameters)
 * ``training_pairs``    views + plain RL-N targets on the GPU
