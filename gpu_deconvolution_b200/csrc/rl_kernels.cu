@@ -585,6 +585,25 @@ struct ColTile {
     };
 };
 
+// Interleaved (float2) column tile for 32-lane groups and 8 columns: element
+// (y, c) at y * 8 + (c ^ ((y >> 1) & 7)).  Sixteen consecutive rows of one
+// column then fall in sixteen distinct 8-byte slots of a 128-byte window, so
+// the per-column reads and both transpose phases (positions XOR-swizzled by
+// tpos) are free of bank conflicts with 64-bit accesses.
+struct ColTile2 {
+    static __device__ __forceinline__ int at(int y, int c) { return y * 8 + (c ^ ((y >> 1) & 7)); }
+    struct ColumnAddr {
+        int c;
+        __device__ __forceinline__ int operator()(int p) const { return at(p, c); }
+    };
+};
+
+__device__ __forceinline__ void cp_async8(void *dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+
 // Column pass for H <= 1024: CW warps per block, G = 32 / T columns per
 // warp, FC = CW * G columns per block.  The FC-column tile is loaded into
 // shared memory with coalesced accesses, each group transforms its column in
@@ -597,13 +616,59 @@ __global__ void __launch_bounds__(CW * 32, FMVD_COL_MIN_BLOCKS) col_pass_w(const
     using WF = WarpFft<H>;
     constexpr int T = WF::T, E = WF::E, G = 32 / T, FC = CW * G, NT = CW * 32;
     using TL = ColTile<T, FC>;
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) float smem[];
     float *tre = smem;
     float *tim = smem + H * TL::ld;
     const int W = a.W;
     const int p = blockIdx.y;
     const int x0 = blockIdx.x * FC;
     float2 *C = a.C + (size_t)p * H * W + x0;
+
+    if constexpr (T == 32 && FC == 8) {
+        // interleaved tile, filled asynchronously
+        float2 *tile = reinterpret_cast<float2 *>(smem);
+#pragma unroll 8
+        for (int u = threadIdx.x; u < H * 8; u += NT) {
+            const int y = u >> 3, c = u & 7;
+            cp_async8(tile + ColTile2::at(y, c), C + (size_t)y * W + c);
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads();
+        const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
+        const ColTile2::ColumnAddr addr{warp};
+        float2 v[E];
+#pragma unroll
+        for (int m = 0; m < E; m++)
+            v[m] = tile[addr(t + T * m)];
+        const float2 *sp = a.spec + (size_t)blockIdx.x * E * NT + threadIdx.x;
+#pragma unroll 1
+        for (int pass = 0; pass < 2; pass++) {
+            WF::template run_addr2<-1>(v, a.tw, tile, t, addr);
+            if (pass == 1)
+                break;
+#pragma unroll
+            for (int m0 = 0; m0 < E; m0 += 8) {
+                asm volatile("" ::: "memory");
+#pragma unroll
+                for (int m = m0; m < m0 + 8 && m < E; m++) {
+                    const float2 z = cmul(v[m], __ldg(sp + (size_t)m * NT));
+                    v[m] = make_float2(z.x, -z.y);
+                }
+            }
+            asm volatile("" ::: "memory");
+        }
+#pragma unroll
+        for (int m = 0; m < E; m++)
+            tile[addr(t + T * m)] = make_float2(v[m].x, -v[m].y);
+        __syncthreads();
+#pragma unroll 4
+        for (int u = threadIdx.x; u < H * 4; u += NT) {
+            const int y = u >> 2, c = 2 * (u & 3);
+            const float2 e0 = tile[ColTile2::at(y, c)], e1 = tile[ColTile2::at(y, c + 1)];
+            *reinterpret_cast<float4 *>(C + (size_t)y * W + c) = make_float4(e0.x, e0.y, e1.x, e1.y);
+        }
+        return;
+    }
 
     constexpr int units = H * FC / 2;
 #pragma unroll 4

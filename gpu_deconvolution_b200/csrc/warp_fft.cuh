@@ -231,6 +231,31 @@ struct WarpFft {
         reorder(v);
     }
 
+    // Same, with the transpose element p at buf[addr(p)] (float2).
+    template <int DIR, typename Addr>
+    static __device__ __forceinline__ void run_addr2(float2 *v, const float2 *__restrict__ tw, float2 *buf, int t,
+                                                     const Addr &addr)
+    {
+        Dft<E, DIR>::run(v);
+        twiddle<DIR>(v, tw, t);
+#pragma unroll
+        for (int k1 = 0; k1 < E; k1++)
+            buf[addr(tpos(k1, t))] = v[k1];
+        __syncwarp();
+#pragma unroll
+        for (int s = 0; s < S; s++) {
+            const int k1 = t + T * s;
+#pragma unroll
+            for (int j = 0; j < T; j++)
+                v[s * T + j] = buf[addr(tpos(k1, j))];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int s = 0; s < S; s++)
+            Dft<T, DIR>::run(v + s * T);
+        reorder(v);
+    }
+
     // Same, with the transpose buffer element p at bre[addr(p)] / bim[addr(p)].
     template <int DIR, typename Addr>
     static __device__ __forceinline__ void run_addr(float2 *v, const float2 *__restrict__ tw, float *bre, float *bim,
