@@ -373,6 +373,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
     constexpr int T = WF::T, E = WF::E, G = 32 / T;
     extern __shared__ __align__(16) float smem[];
     __shared__ __align__(8) uint64_t bars[kRowWarps * G];
+    __shared__ __align__(8) uint64_t ebars[MODE == ROW_UPDATE ? kRowWarps * G : 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane / T, t = lane % T;
     const int gi = warp * G + g;
@@ -388,25 +389,30 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
     RowWork<MODE> work(a, p, y);
 
     // Rows the element-wise step needs are fetched by the bulk-copy engine
-    // while the inverse transform runs: the estimate and weight rows in the
-    // update pass, the two data rows in the divide pass.
-    const bool prefetch = MODE == ROW_UPDATE || (MODE == ROW_DIVIDE && a.bulk_data);
+    // while the inverse transform runs: the weight row in the update pass,
+    // the two data rows in the divide pass.  The update pass's estimate row
+    // lands in the transpose buffer itself, issued once the inverse
+    // transform has read its transpose back, so it takes no shared memory
+    // of its own.
+    const bool prefetch = (MODE == ROW_UPDATE && a.bulk_weights) || (MODE == ROW_DIVIDE && a.bulk_data);
     uint64_t *bar = &bars[gi];
-    if (prefetch) {
+    uint64_t *ebar = &ebars[MODE == ROW_UPDATE ? gi : 0];
+    if (prefetch || MODE == ROW_UPDATE) {
         if (t == 0) {
             mbar_init(bar, 1);
+            if (MODE == ROW_UPDATE)
+                mbar_init(ebar, 1);
             mbar_fence_init();
         }
         __syncwarp();
+    }
+    if (prefetch) {
         if (t == 0) {
             const int es = a.d.bits == 16 ? 2 : 1;
             if (MODE == ROW_UPDATE) {
-                const uint32_t eb = W * sizeof(float2);
-                const uint32_t wb = a.bulk_weights ? a.d.dataW * sizeof(float) : 0;
-                mbar_arrive_expect_tx(bar, eb + wb);
-                bulk_load(pf, work.est, eb, bar);
-                if (wb)
-                    bulk_load(pf + eb, work.wrow, wb, bar);
+                const uint32_t wb = a.d.dataW * sizeof(float);
+                mbar_arrive_expect_tx(bar, wb);
+                bulk_load(pf, work.wrow, wb, bar);
             } else {
                 const uint32_t rb = a.d.dataW * es;
                 const uint32_t rs = (rb + 15) & ~15u;
@@ -433,8 +439,16 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
                 work.apply(t + T * m, v[m]);
         }
     }
+    int pass = MODE == ROW_INIT ? 1 : 0;
+    const auto estimate_to_tbuf = [&]() {
+        if (MODE == ROW_UPDATE && pass == 0 && t == 0) {
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(ebar, W * sizeof(float2));
+            bulk_load(tbuf, work.est, W * sizeof(float2), ebar);
+        }
+    };
 #pragma unroll 1
-    for (int pass = (MODE == ROW_INIT ? 1 : 0); pass < 2; pass++) {
+    for (; pass < 2; pass++) {
         if (pass == 0) {
 #pragma unroll
             for (int m = 0; m < E; m++) {
@@ -442,25 +456,38 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
                 v[m] = make_float2(x.x, -x.y);
             }
         }
-        WF::template run_padded<-1>(v, a.tw, tbuf, t);
+        WF::template run_padded<-1>(v, a.tw, tbuf, t, estimate_to_tbuf);
         if (pass == 1)
             break;
 #pragma unroll
         for (int m = 0; m < E; m++)
             v[m].y = -v[m].y;
-    if (prefetch) {
+    if (MODE == ROW_UPDATE) {
+        const bool ok_w = !prefetch || mbar_wait(bar, 0);
+        const bool ok_e = mbar_wait(ebar, 0);
+        if (!ok_w || !ok_e) {
+            // a copy did not land in time: flag it, wait once more so no copy
+            // is left in flight, and continue from global memory
+            if (t == 0)
+                atomicExch(a.b.status, 1);
+            if (!ok_w)
+                mbar_wait(bar, 0);
+            if (!ok_e)
+                mbar_wait(ebar, 0);
+        } else {
+            work.est_s = tbuf;
+            if (prefetch) {
+                work.wrow = reinterpret_cast<const float *>(pf);
+                work.w_s = true;
+            }
+        }
+    } else if (prefetch) {
         if (!mbar_wait(bar, 0)) {
             // the copy did not land in time: flag it, wait once more so no copy
             // is left in flight, and continue from global memory
             if (t == 0)
                 atomicExch(a.b.status, 1);
             mbar_wait(bar, 0);
-        } else if (MODE == ROW_UPDATE) {
-            work.est_s = reinterpret_cast<const float2 *>(pf);
-            if (a.bulk_weights) {
-                work.wrow = reinterpret_cast<const float *>(pf + W * sizeof(float2));
-                work.w_s = true;
-            }
         } else {
             const int es = a.d.bits == 16 ? 2 : 1;
             const uint32_t rs = (a.d.dataW * es + 15) & ~15u;
@@ -476,6 +503,8 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
     }
     if (MODE == ROW_UPDATE && a.last)
         return;
+    if (MODE == ROW_UPDATE)
+        __syncwarp();  // the estimate row in tbuf is read before the forward transform writes it
     }
     if (valid) {
 #pragma unroll
@@ -955,9 +984,10 @@ static void launch_row(const RowArgs &a0, cudaStream_t s)
                          ((size_t)a.d.dataH * a.d.dataW * sizeof(float)) % 16 == 0;
         size_t pf = 0;
         if (MODE == ROW_UPDATE)
-            pf = W * sizeof(float2) + (a.bulk_weights ? a.d.dataW * sizeof(float) : 0);
+            pf = a.bulk_weights ? a.d.dataW * sizeof(float) : 0;
         else if (MODE == ROW_DIVIDE && a.bulk_data)
             pf = 2 * ((a.d.dataW * es + 15) & ~(size_t)15);
+        static_assert(WF::padded_f2 >= W, "the update pass lands the estimate row in the transpose buffer");
         a.group_floats = WF::padded_floats + (int)(pf / sizeof(float));
         const size_t smem = sizeof(float) * kRowWarps * G * (size_t)a.group_floats;
         auto kern = row_pass_w<W, MODE>;

@@ -17,6 +17,10 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
 // Makes barrier initialisation visible to the asynchronous (TMA) proxy.
 __device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
+// Orders this thread's earlier shared-memory accesses before bulk copies it
+// issues afterwards (generic and asynchronous proxy).
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32addr(bar)), "r"(bytes)

@@ -207,9 +207,16 @@ struct WarpFft {
     static constexpr int padded_f2 = E * (T + 1);
     static constexpr int padded_floats = ((2 * padded_f2 + 3) / 4) * 4;  // 16-byte multiple
 
+    struct Nothing {
+        __device__ __forceinline__ void operator()() const {}
+    };
+
     // The transform with the transpose through the padded float2 buffer buf.
-    template <int DIR>
-    static __device__ __forceinline__ void run_padded(float2 *v, const float2 *__restrict__ tw, float2 *buf, int t)
+    // after_read() runs once every lane has read its transpose elements back,
+    // when buf is free for other use until the next transform.
+    template <int DIR, typename AfterRead = Nothing>
+    static __device__ __forceinline__ void run_padded(float2 *v, const float2 *__restrict__ tw, float2 *buf, int t,
+                                                      const AfterRead &after_read = AfterRead())
     {
         Dft<E, DIR>::run(v);
         twiddle<DIR>(v, tw, t);
@@ -225,6 +232,7 @@ struct WarpFft {
             for (int j = 0; j < T; j++)
                 v[s * T + j] = rd[s * T * (T + 1) + j];
         __syncwarp();
+        after_read();
 #pragma unroll
         for (int s = 0; s < S; s++)
             Dft<T, DIR>::run(v + s * T);
