@@ -627,6 +627,47 @@ struct ColTile2 {
     };
 };
 
+// float2 shared-memory access by 32-bit shared-window address.
+__device__ __forceinline__ void sts2(uint32_t addr, float2 v)
+{
+    asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
+}
+__device__ __forceinline__ float2 lds2(uint32_t addr)
+{
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr) : "memory");
+    return v;
+}
+
+// Byte addresses in a ColTile2 tile that starts on a 2048-byte boundary.
+// Slot (y, c) sits at byte 64 y + 8 (c ^ ((y >> 1) & 7)); for y = 32 a + u,
+// u < 32, that is 2048 a + Q_c(u) with Q_c(u) = 64 u + 8 (c ^ ((u >> 1) & 7)).
+// Q_c is XOR-linear: Q_c(t ^ k) = Q_c(t) ^ R(k), R(k) = 64 k + 8 ((k >> 1) & 7),
+// so every transpose address of the 1024-point column transform is a lane
+// constant XOR a compile-time constant (one logic instruction) plus an
+// immediate offset.
+__host__ __device__ constexpr uint32_t coltile_r(int k) { return 64u * k + 8u * ((k >> 1) & 7); }
+
+// 1024-point transform of one tile column (the WarpFft<1024> four-step with
+// T = E = 32): wbase = tile | Q_c(t) (transpose writes, element k1 at row
+// 32 k1 + (t ^ k1)), rbase = (tile + 2048 t) | Q_c(t) (reads of row-block t).
+template <int DIR>
+__device__ __forceinline__ void col_fft_1024(float2 *v, const float2 *__restrict__ tw, uint32_t wbase,
+                                             uint32_t rbase, int t)
+{
+    Dft<32, DIR>::run(v);
+    WarpFft<1024>::twiddle<DIR>(v, tw, t);
+#pragma unroll
+    for (int k1 = 0; k1 < 32; k1++)
+        sts2((wbase ^ coltile_r(k1)) + 2048u * k1, v[k1]);
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 32; j++)
+        v[j] = lds2(rbase ^ coltile_r(j));
+    __syncwarp();
+    Dft<32, DIR>::run(v);
+}
+
 __device__ __forceinline__ void cp_async8(void *dst, const void *src)
 {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
@@ -654,8 +695,11 @@ __global__ void __launch_bounds__(CW * 32, FMVD_COL_MIN_BLOCKS) col_pass_w(const
     float2 *C = a.C + (size_t)p * H * W + x0;
 
     if constexpr (T == 32 && FC == 8) {
-        // interleaved tile, filled asynchronously
-        float2 *tile = reinterpret_cast<float2 *>(smem);
+        static_assert(H == 1024, "the interleaved tile path is the 1024-point column transform");
+        // interleaved tile on a 2048-byte boundary, filled asynchronously
+        const uint32_t s0 = smem_u32addr(smem);
+        const uint32_t base = (s0 + 2047u) & ~2047u;
+        float2 *tile = reinterpret_cast<float2 *>(reinterpret_cast<char *>(smem) + (base - s0));
 #pragma unroll 8
         for (int u = threadIdx.x; u < H * 8; u += NT) {
             const int y = u >> 3, c = u & 7;
@@ -664,15 +708,16 @@ __global__ void __launch_bounds__(CW * 32, FMVD_COL_MIN_BLOCKS) col_pass_w(const
         asm volatile("cp.async.wait_all;" ::: "memory");
         __syncthreads();
         const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
-        const ColTile2::ColumnAddr addr{warp};
+        const uint32_t q = 64u * t + 8u * (warp ^ ((t >> 1) & 7));
+        const uint32_t wbase = base | q, rbase = (base + 2048u * t) | q;
         float2 v[E];
 #pragma unroll
         for (int m = 0; m < E; m++)
-            v[m] = tile[addr(t + T * m)];
+            v[m] = lds2(wbase + 2048u * m);  // row t + 32 m
         const float2 *sp = a.spec + (size_t)blockIdx.x * E * NT + threadIdx.x;
 #pragma unroll 1
         for (int pass = 0; pass < 2; pass++) {
-            WF::template run_addr2<-1>(v, a.tw, tile, t, addr);
+            col_fft_1024<-1>(v, a.tw, wbase, rbase, t);
             if (pass == 1)
                 break;
 #pragma unroll
@@ -688,7 +733,7 @@ __global__ void __launch_bounds__(CW * 32, FMVD_COL_MIN_BLOCKS) col_pass_w(const
         }
 #pragma unroll
         for (int m = 0; m < E; m++)
-            tile[addr(t + T * m)] = make_float2(v[m].x, -v[m].y);
+            sts2(wbase + 2048u * m, make_float2(v[m].x, -v[m].y));
         __syncthreads();
 #pragma unroll 4
         for (int u = threadIdx.x; u < H * 4; u += NT) {
@@ -1024,7 +1069,8 @@ static void launch_col_w(const ColArgs &a, int npairs, cudaStream_t s)
 {
     using WF = WarpFft<H>;
     constexpr int FC = CW * (32 / WF::T);
-    constexpr size_t smem = sizeof(float) * 2 * H * ColTile<WF::T, FC>::ld;
+    // the interleaved-tile path (T = 32, 8 columns) aligns its tile to 2048 bytes
+    constexpr size_t smem = sizeof(float) * 2 * H * ColTile<WF::T, FC>::ld + (WF::T == 32 && FC == 8 ? 2048 : 0);
     auto kern = col_pass_w<H, CW>;
     static unsigned mask = 0;
     configure_smem(kern, smem, mask);
