@@ -131,17 +131,18 @@ std::vector<double2> twiddles_d(int n)
 }
 
 // Twiddle table of the warp FFT's four-step split N = T x E (zeros when N
-// has no warp split): with R8 = min(E, 8) and J = E / R8,
+// has no warp split), rl_warp_twiddle_entries(N) entries: with
+// R8 = min(E, kWarpTwiddleRun) and J = E / R8,
 //   [j * T + t] = exp(-2 pi i R8 j t / N) for j < J, t < T
 //   [J * T + t] = exp(-2 pi i t / N)
 std::vector<float2> warp_twiddles(int n)
 {
-    std::vector<float2> t(n, make_float2(0.f, 0.f));
+    std::vector<float2> t(rl_warp_twiddle_entries(n), make_float2(0.f, 0.f));
     const int T = rl_warp_lanes(n);
     if (T == 0)
         return t;
     const int E = n / T;
-    const int R8 = E < 8 ? E : 8;
+    const int R8 = E < kWarpTwiddleRun ? E : kWarpTwiddleRun;
     const int J = E / R8;
     auto w = [n](long long k) {
         const double a = -2.0 * M_PI * (double)(k % n) / (double)n;
@@ -244,7 +245,8 @@ Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weig
               FMVD_CHECK(cudaMalloc(&e->C, sizeof(float2) * (size_t)H * W * e->pairs_cap)) &&
               FMVD_CHECK(cudaMalloc(&e->est, sizeof(float2) * (size_t)H * W * e->pairs_cap)) &&
               FMVD_CHECK(cudaMalloc(&e->twH, sizeof(float2) * H)) && FMVD_CHECK(cudaMalloc(&e->twW, sizeof(float2) * W)) &&
-              FMVD_CHECK(cudaMalloc(&e->wtwH, sizeof(float2) * H)) && FMVD_CHECK(cudaMalloc(&e->wtwW, sizeof(float2) * W)) &&
+              FMVD_CHECK(cudaMalloc(&e->wtwH, sizeof(float2) * rl_warp_twiddle_entries(H))) &&
+              FMVD_CHECK(cudaMalloc(&e->wtwW, sizeof(float2) * rl_warp_twiddle_entries(W))) &&
               FMVD_CHECK(cudaMalloc(&e->status, sizeof(int))) && FMVD_CHECK(cudaMemset(e->status, 0, sizeof(int)));
     if (ok && e->lanes > 1)
         ok = FMVD_CHECK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
@@ -269,8 +271,8 @@ Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weig
         std::vector<float2> wH = warp_twiddles(H), wW = warp_twiddles(W);
         ok = FMVD_CHECK(cudaMemcpy(e->twH, fH.data(), sizeof(float2) * H, cudaMemcpyHostToDevice)) &&
              FMVD_CHECK(cudaMemcpy(e->twW, fW.data(), sizeof(float2) * W, cudaMemcpyHostToDevice)) &&
-             FMVD_CHECK(cudaMemcpy(e->wtwH, wH.data(), sizeof(float2) * H, cudaMemcpyHostToDevice)) &&
-             FMVD_CHECK(cudaMemcpy(e->wtwW, wW.data(), sizeof(float2) * W, cudaMemcpyHostToDevice));
+             FMVD_CHECK(cudaMemcpy(e->wtwH, wH.data(), sizeof(float2) * wH.size(), cudaMemcpyHostToDevice)) &&
+             FMVD_CHECK(cudaMemcpy(e->wtwW, wW.data(), sizeof(float2) * wW.size(), cudaMemcpyHostToDevice));
 
         // kernel spectra
         double2 *d_twH = nullptr, *d_twW = nullptr, *work = nullptr;

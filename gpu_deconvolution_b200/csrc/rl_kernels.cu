@@ -1145,6 +1145,16 @@ void rl_col(const RlDims &d, const RlBatch &b, const RlTables &t, const float2 *
 
 int rl_warp_lanes(int n) { return n <= 1024 ? warp_fft_lanes(n) : 0; }
 
+int rl_warp_twiddle_entries(int n)
+{
+    const int T = rl_warp_lanes(n);
+    if (T == 0)
+        return n;
+    const int E = n / T, R = E < kWarpTwiddleRun ? E : kWarpTwiddleRun;
+    const int used = (E / R + 1) * T;
+    return used > n ? used : n;
+}
+
 void rl_kernel_spectrum(const float *d_kernel, int kH, int kW, int H, int W, const double2 *twH, const double2 *twW,
                         double2 *work, float2 *d_out, int cw, cudaStream_t s)
 {

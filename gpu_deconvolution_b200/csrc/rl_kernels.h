@@ -41,12 +41,17 @@ struct RlBatch {
 struct RlTables {
     const float2 *twH;   // exp(-2 pi i n / H)            (lengths above 1024)
     const float2 *twW;   // exp(-2 pi i n / W)
-    const float2 *wtwH;  // warp-FFT twiddles of H: [k1 * T + t] = exp(-2 pi i t k1 / H)   (lengths <= 1024)
+    const float2 *wtwH;  // warp-FFT twiddles of H (lengths <= 1024; layout in warp_twiddles)
     const float2 *wtwW;  // warp-FFT twiddles of W
 };
 
 // Lanes per line of the warp FFT for length n (0 when n > 1024).
 int rl_warp_lanes(int n);
+// Twiddle run of the warp FFT: lane t forms w_N^(t k1), k1 = R j + b, as the
+// table entry w_N^(R j t) times (w_N^t)^b, b < R (R = min(E, this)).
+constexpr int kWarpTwiddleRun = 2;
+// float2 entries of the warp-FFT twiddle table of length n (at least n).
+int rl_warp_twiddle_entries(int n);
 // Column-pass warps per block for an H x W plane: 'requested' (2, 4 or 8)
 // when the plane allows it, the widest allowed when 0, -1 when not allowed.
 int rl_col_warps(int H, int W, int requested);

@@ -16,6 +16,7 @@
 #pragma once
 
 #include "fft_engine.cuh"
+#include "rl_kernels.h"
 
 namespace fmvd {
 
@@ -132,12 +133,12 @@ struct WarpFft {
     static __device__ __forceinline__ int tpos(int k1, int t) { return k1 * T + (t ^ (k1 & (T - 1))); }
 
     // Twiddle table layout (per length N, built on the host, float2):
-    //   [j * T + t]       = w_N^(R8 j t)   for j < J   (R8 = min(E, 8), J = E / R8)
+    //   [j * T + t]       = w_N^(R8 j t)   for j < J   (R8 = min(E, kWarpTwiddleRun), J = E / R8)
     //   [J * T + t]       = w_N^t
     // Lane t forms w_N^(t k1), k1 = R8 j + b, as table[j] * (w_N^t)^b with the
     // powers b < R8 by repeated multiplication: J + 1 loads per transform
     // instead of E - 1, and at most R8 rounding steps per twiddle.
-    static constexpr int R8 = E < 8 ? E : 8;
+    static constexpr int R8 = E < kWarpTwiddleRun ? E : kWarpTwiddleRun;
     static constexpr int J = E / R8;
     static constexpr int table_size = (J + 1) * T;
 
