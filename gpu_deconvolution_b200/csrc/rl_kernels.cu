@@ -139,7 +139,11 @@ __device__ __forceinline__ void store_sample(void *base, size_t idx, float v, in
 //           reference's in-place quirk)
 //   UPDATE: correction r -> e + w (e r - e) (multiply32_kernel); after the
 //           last view of the last iteration also the output samples
-template <int MODE>
+// BITS: the sample width when fixed at compile time (8 or 16), else 0.  With
+// it fixed, operand rows are read through generic pointers that may point to
+// shared or global memory, so the element-wise step has no per-element
+// branches.
+template <int MODE, int BITS = 0>
 struct RowWork {
     const RlDims &d;
     float2 *est;             // row y of the pair's estimate (global)
@@ -188,6 +192,10 @@ struct RowWork {
 
     __device__ __forceinline__ float sample(const void *row, int sx) const
     {
+        if constexpr (BITS == 16)
+            return (float)reinterpret_cast<const unsigned short *>(row)[sx];
+        else if constexpr (BITS == 8)
+            return (float)reinterpret_cast<const unsigned char *>(row)[sx];
         if (src_s)
             return d.bits == 16 ? (float)reinterpret_cast<const unsigned short *>(row)[sx]
                                 : (float)reinterpret_cast<const unsigned char *>(row)[sx];
@@ -212,17 +220,24 @@ struct RowWork {
             v = q;
         } else {
             const int sx = clamp_src(x, d.dataW, d.bxW);
-            const float w = w_s ? wrow[sx] : __ldg(wrow + sx);
-            float2 c = est_s ? est_s[x] : __ldcs(est + x);
+            float w;
+            float2 c;
+            if constexpr (BITS != 0) {
+                w = wrow[sx];
+                c = (est_s ? est_s : est)[x];
+            } else {
+                w = w_s ? wrow[sx] : __ldg(wrow + sx);
+                c = est_s ? est_s[x] : __ldcs(est + x);
+            }
             const float2 r = v;
             c.x += w * (c.x * r.x - c.x);
             c.y += w * (c.y * r.y - c.y);
             __stcs(est + x, c);
             v = c;
             if (out0 && x < d.dataW) {
-                store_sample(out0, x, c.x, d.bits);
+                store_sample(out0, x, c.x, BITS ? BITS : d.bits);
                 if (out1)
-                    store_sample(out1, x, c.y, d.bits);
+                    store_sample(out1, x, c.y, BITS ? BITS : d.bits);
             }
         }
     }
@@ -366,7 +381,7 @@ __global__ void __launch_bounds__(Cfg<W, F>::NT, FMVD_BLOCK_ROW_MIN_BLOCKS) row_
 #endif
 constexpr int kRowWarps = 4;
 
-template <int W, int MODE>
+template <int W, int MODE, int BITS>
 __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_w(const RowArgs a)
 {
     using WF = WarpFft<W>;
@@ -386,7 +401,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
     const int y = valid ? yr : H - 1;
     const int p = blockIdx.y;
     float2 *row = a.b.C + ((size_t)p * H + y) * W;
-    RowWork<MODE> work(a, p, y);
+    RowWork<MODE, BITS> work(a, p, y);
 
     // Rows the element-wise step needs are fetched by the bulk-copy engine
     // while the inverse transform runs: the weight row in the update pass,
@@ -1035,9 +1050,21 @@ static void launch_row(const RowArgs &a0, cudaStream_t s)
         static_assert(WF::padded_f2 >= W, "the update pass lands the estimate row in the transpose buffer");
         a.group_floats = WF::padded_floats + (int)(pf / sizeof(float));
         const size_t smem = sizeof(float) * kRowWarps * G * (size_t)a.group_floats;
-        auto kern = row_pass_w<W, MODE>;
-        static unsigned mask = 0;
-        configure_smem(kern, 200 * 1024, mask);
+        // the element-wise step is compiled for the sample width
+        void (*kern)(const RowArgs);
+        static unsigned mask[3] = {0, 0, 0};
+        unsigned *m;
+        if constexpr (MODE == ROW_INIT) {
+            kern = row_pass_w<W, MODE, 0>;
+            m = &mask[0];
+        } else if (a.d.bits == 16) {
+            kern = row_pass_w<W, MODE, 16>;
+            m = &mask[1];
+        } else {
+            kern = row_pass_w<W, MODE, 8>;
+            m = &mask[2];
+        }
+        configure_smem(kern, 200 * 1024, *m);
         dim3 grid((a.d.H + kRowWarps * G - 1) / (kRowWarps * G), a.b.npairs);
         kern<<<grid, kRowWarps * 32, smem, s>>>(a);
     } else {
