@@ -243,10 +243,10 @@ struct RowWork {
     }
 };
 
-template <int MODE>
+template <int MODE, int BITS>
 __device__ __forceinline__ void pointwise(const RowArgs &a, int p, int y, int x, float2 &v)
 {
-    RowWork<MODE>(a, p, y).apply(x, v);
+    RowWork<MODE, BITS>(a, p, y).apply(x, v);
 }
 
 // Row pass for W > 1024: F rows per block through the shared-memory Stockham engine.
@@ -265,7 +265,7 @@ struct BlockRowPrefetch {
     static __host__ __device__ size_t row_bytes(size_t b) { return (b + 15) & ~(size_t)15; }
 };
 
-template <int W, int F, int MODE>
+template <int W, int F, int MODE, int BITS>
 __global__ void __launch_bounds__(Cfg<W, F>::NT, FMVD_BLOCK_ROW_MIN_BLOCKS) row_pass(const RowArgs a)
 {
     extern __shared__ __align__(16) float smem[];
@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(Cfg<W, F>::NT, FMVD_BLOCK_ROW_MIN_BLOCKS) row_
         // thread's slots usually all lie in one row)
         int f0, x0;
         EG::pos(0, f0, x0);
-        RowWork<MODE> w0(a, p, y0 + f0);
+        RowWork<MODE, BITS> w0(a, p, y0 + f0);
         if (prefetch) {
             if (!mbar_wait(&pbar, 0)) {
                 // the copies did not land in time: flag it, wait once more so
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(Cfg<W, F>::NT, FMVD_BLOCK_ROW_MIN_BLOCKS) row_
             if (f == f0)
                 w0.apply(x, v[e]);
             else
-                pointwise<MODE>(a, p, y0 + f, x, v[e]);
+                pointwise<MODE, BITS>(a, p, y0 + f, x, v[e]);
         }
     }
     if (MODE == ROW_UPDATE && a.last)
@@ -1082,9 +1082,20 @@ static void launch_row(const RowArgs &a0, cudaStream_t s)
         else if (MODE == ROW_DIVIDE && a.bulk_data)
             pf = 2 * F * PF::row_bytes(a.d.dataW * es);
         const size_t smem = PF::offset + pf;
-        auto kern = row_pass<W, F, MODE>;
-        static unsigned mask = 0;
-        configure_smem(kern, 200 * 1024, mask);
+        void (*kern)(const RowArgs);
+        static unsigned mask[3] = {0, 0, 0};
+        unsigned *m;
+        if constexpr (MODE == ROW_INIT) {
+            kern = row_pass<W, F, MODE, 0>;
+            m = &mask[0];
+        } else if (a.d.bits == 16) {
+            kern = row_pass<W, F, MODE, 16>;
+            m = &mask[1];
+        } else {
+            kern = row_pass<W, F, MODE, 8>;
+            m = &mask[2];
+        }
+        configure_smem(kern, 200 * 1024, *m);
         dim3 grid(a.d.H / F, a.b.npairs);
         kern<<<grid, Cfg<W, F>::NT, smem, s>>>(a);
     }
