@@ -46,7 +46,9 @@ __host__ __device__ __forceinline__ size_t tile_index(int y, int x, int W) { ret
 
 __device__ __forceinline__ int clamp_src(int i, int n, int border)
 {
-    return i < n ? i : (i < n + border ? n - 1 : 0);
+    // i < n: i; n <= i < n + border: n - 1; beyond: 0 (i >= 0)
+    const int c = min(i, n - 1);
+    return i < n + border ? c : 0;
 }
 
 // Rows per row-pass block and columns per column-pass block.
@@ -142,8 +144,9 @@ __device__ __forceinline__ void store_sample(void *base, size_t idx, float v, in
 // BITS: the sample width when fixed at compile time (8 or 16), else 0.  With
 // it fixed, operand rows are read through generic pointers that may point to
 // shared or global memory, so the element-wise step has no per-element
-// branches.
-template <int MODE, int BITS = 0>
+// branches.  NOOUT: an update pass known at compile time not to be the last
+// one, so the output-sample code is left out.
+template <int MODE, int BITS = 0, bool NOOUT = false>
 struct RowWork {
     const RlDims &d;
     float2 *est;             // row y of the pair's estimate (global)
@@ -234,7 +237,7 @@ struct RowWork {
             c.y += w * (c.y * r.y - c.y);
             __stcs(est + x, c);
             v = c;
-            if (out0 && x < d.dataW) {
+            if (!NOOUT && out0 && x < d.dataW) {
                 store_sample(out0, x, c.x, BITS ? BITS : d.bits);
                 if (out1)
                     store_sample(out1, x, c.y, BITS ? BITS : d.bits);
@@ -381,7 +384,7 @@ __global__ void __launch_bounds__(Cfg<W, F>::NT, FMVD_BLOCK_ROW_MIN_BLOCKS) row_
 #endif
 constexpr int kRowWarps = 4;
 
-template <int W, int MODE, int BITS>
+template <int W, int MODE, int BITS, bool NOOUT>
 __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_w(const RowArgs a)
 {
     using WF = WarpFft<W>;
@@ -401,7 +404,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
     const int y = valid ? yr : H - 1;
     const int p = blockIdx.y;
     float2 *row = a.b.C + ((size_t)p * H + y) * W;
-    RowWork<MODE, BITS> work(a, p, y);
+    RowWork<MODE, BITS, NOOUT> work(a, p, y);
 
     // Rows the element-wise step needs are fetched by the bulk-copy engine
     // while the inverse transform runs: the weight row in the update pass,
@@ -516,7 +519,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
         for (int m = 0; m < E; m++)
             work.apply(t + T * m, v[m]);
     }
-    if (MODE == ROW_UPDATE && a.last)
+    if (MODE == ROW_UPDATE && !NOOUT && a.last)
         return;
     if (MODE == ROW_UPDATE)
         __syncwarp();  // the estimate row in tbuf is read before the forward transform writes it
@@ -1051,18 +1054,20 @@ static void launch_row(const RowArgs &a0, cudaStream_t s)
         a.group_floats = WF::padded_floats + (int)(pf / sizeof(float));
         const size_t smem = sizeof(float) * kRowWarps * G * (size_t)a.group_floats;
         // the element-wise step is compiled for the sample width
+        // compiled per sample width, and for the update pass per last / not last
         void (*kern)(const RowArgs);
-        static unsigned mask[3] = {0, 0, 0};
+        static unsigned mask[5] = {0, 0, 0, 0, 0};
         unsigned *m;
+        const bool noout = MODE == ROW_UPDATE && !a.last;
         if constexpr (MODE == ROW_INIT) {
-            kern = row_pass_w<W, MODE, 0>;
+            kern = row_pass_w<W, MODE, 0, false>;
             m = &mask[0];
         } else if (a.d.bits == 16) {
-            kern = row_pass_w<W, MODE, 16>;
-            m = &mask[1];
+            kern = noout ? row_pass_w<W, MODE, 16, MODE == ROW_UPDATE> : row_pass_w<W, MODE, 16, false>;
+            m = &mask[noout ? 3 : 1];
         } else {
-            kern = row_pass_w<W, MODE, 8>;
-            m = &mask[2];
+            kern = noout ? row_pass_w<W, MODE, 8, MODE == ROW_UPDATE> : row_pass_w<W, MODE, 8, false>;
+            m = &mask[noout ? 4 : 2];
         }
         configure_smem(kern, 200 * 1024, *m);
         dim3 grid((a.d.H + kRowWarps * G - 1) / (kRowWarps * G), a.b.npairs);
