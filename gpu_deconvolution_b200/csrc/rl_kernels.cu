@@ -51,6 +51,30 @@ __device__ __forceinline__ int clamp_src(int i, int n, int border)
     return i < n + border ? c : 0;
 }
 
+// Shared-memory loads by 32-bit shared-window address.
+__device__ __forceinline__ float lds_f32(uint32_t addr)
+{
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr) : "memory");
+    return v;
+}
+__device__ __forceinline__ float2 lds_f32x2(uint32_t addr)
+{
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr) : "memory");
+    return v;
+}
+template <int BITS>
+__device__ __forceinline__ float lds_sample(uint32_t row, int sx)
+{
+    uint32_t v;
+    if constexpr (BITS == 16)
+        asm volatile("ld.shared.u16 %0, [%1];" : "=r"(v) : "r"(row + 2u * sx) : "memory");
+    else
+        asm volatile("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(row + (uint32_t)sx) : "memory");
+    return (float)v;
+}
+
 // Rows per row-pass block and columns per column-pass block.
 __host__ __device__ constexpr int row_f(int W) { return W <= 1024 ? 2048 / W : 2; }
 __host__ __device__ constexpr int col_f(int H) { return H <= 256 ? 2048 / H : (H <= 1024 ? 8 : 4); }
@@ -145,8 +169,10 @@ __device__ __forceinline__ void store_sample(void *base, size_t idx, float v, in
 // it fixed, operand rows are read through generic pointers that may point to
 // shared or global memory, so the element-wise step has no per-element
 // branches.  NOOUT: an update pass known at compile time not to be the last
-// one, so the output-sample code is left out.
-template <int MODE, int BITS = 0, bool NOOUT = false>
+// one, so the output-sample code is left out.  SMEM (with BITS fixed): the
+// operand rows are in shared memory at the s_* addresses (the data rows in
+// the divide pass; the estimate and weight rows in the update pass).
+template <int MODE, int BITS = 0, bool NOOUT = false, bool SMEM = false>
 struct RowWork {
     const RlDims &d;
     float2 *est;             // row y of the pair's estimate (global)
@@ -159,6 +185,7 @@ struct RowWork {
     bool has1;
     float init0, init1;
     const float *initr0, *initr1;  // rows of a given initial estimate, or null
+    uint32_t s_src0, s_src1, s_w, s_est;  // shared-memory rows (SMEM)
 
     __device__ __forceinline__ RowWork(const RowArgs &a, int p, int y) : d(a.d)
     {
@@ -215,8 +242,15 @@ struct RowWork {
             // q > 1 keeps the divisor in the range where the fast division is
             // within 2 ulp of the IEEE quotient
             const int sx = clamp_src(x, d.dataW, d.bxD);
-            const float a0 = sample(src0, sx);
-            const float a1 = has1 ? sample(src1, sx) : 0.f;
+            float a0, a1;
+            if constexpr (SMEM) {
+                a0 = lds_sample<BITS>(s_src0, sx);
+                const float s1 = lds_sample<BITS>(s_src1, sx);
+                a1 = has1 ? s1 : 0.f;
+            } else {
+                a0 = sample(src0, sx);
+                a1 = has1 ? sample(src1, sx) : 0.f;
+            }
             float2 q = v;
             q.x = q.x > 1.f ? __fdividef(a0, q.x) : q.x;
             q.y = q.y > 1.f ? __fdividef(a1, q.y) : q.y;
@@ -225,7 +259,10 @@ struct RowWork {
             const int sx = clamp_src(x, d.dataW, d.bxW);
             float w;
             float2 c;
-            if constexpr (BITS != 0) {
+            if constexpr (SMEM) {
+                w = lds_f32(s_w + 4u * sx);
+                c = lds_f32x2(s_est + 8u * x);
+            } else if constexpr (BITS != 0) {
                 w = wrow[sx];
                 c = (est_s ? est_s : est)[x];
             } else {
@@ -384,7 +421,7 @@ __global__ void __launch_bounds__(Cfg<W, F>::NT, FMVD_BLOCK_ROW_MIN_BLOCKS) row_
 #endif
 constexpr int kRowWarps = 4;
 
-template <int W, int MODE, int BITS, bool NOOUT>
+template <int W, int MODE, int BITS, bool NOOUT, bool SMEM>
 __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_w(const RowArgs a)
 {
     using WF = WarpFft<W>;
@@ -404,7 +441,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
     const int y = valid ? yr : H - 1;
     const int p = blockIdx.y;
     float2 *row = a.b.C + ((size_t)p * H + y) * W;
-    RowWork<MODE, BITS, NOOUT> work(a, p, y);
+    RowWork<MODE, BITS, NOOUT, SMEM> work(a, p, y);
 
     // Rows the element-wise step needs are fetched by the bulk-copy engine
     // while the inverse transform runs: the weight row in the update pass,
@@ -412,7 +449,9 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
     // lands in the transpose buffer itself, issued once the inverse
     // transform has read its transpose back, so it takes no shared memory
     // of its own.
-    const bool prefetch = (MODE == ROW_UPDATE && a.bulk_weights) || (MODE == ROW_DIVIDE && a.bulk_data);
+    // SMEM is set exactly when the launch allows the bulk copies (weights in
+    // the update pass, data in the divide pass)
+    constexpr bool prefetch = SMEM && MODE != ROW_INIT;
     uint64_t *bar = &bars[gi];
     uint64_t *ebar = &ebars[MODE == ROW_UPDATE ? gi : 0];
     if (prefetch || MODE == ROW_UPDATE) {
@@ -484,15 +523,20 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
         const bool ok_w = !prefetch || mbar_wait(bar, 0);
         const bool ok_e = mbar_wait(ebar, 0);
         if (!ok_w || !ok_e) {
-            // a copy did not land in time: flag it, wait once more so no copy
-            // is left in flight, and continue from global memory
+            // a copy did not land in time: flag it (the host reports the
+            // batch as failed), wait once more so no copy is left in flight,
+            // and continue from global memory where the code allows it
             if (t == 0)
                 atomicExch(a.b.status, 1);
             if (!ok_w)
                 mbar_wait(bar, 0);
             if (!ok_e)
                 mbar_wait(ebar, 0);
-        } else {
+        }
+        if constexpr (SMEM) {
+            work.s_est = smem_u32addr(tbuf);
+            work.s_w = smem_u32addr(pf);
+        } else if (ok_w && ok_e) {
             work.est_s = tbuf;
             if (prefetch) {
                 work.wrow = reinterpret_cast<const float *>(pf);
@@ -501,18 +545,16 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
         }
     } else if (prefetch) {
         if (!mbar_wait(bar, 0)) {
-            // the copy did not land in time: flag it, wait once more so no copy
-            // is left in flight, and continue from global memory
+            // the copy did not land in time: flag it (the host reports the
+            // batch as failed) and wait once more so no copy is left in flight
             if (t == 0)
                 atomicExch(a.b.status, 1);
             mbar_wait(bar, 0);
-        } else {
-            const int es = a.d.bits == 16 ? 2 : 1;
-            const uint32_t rs = (a.d.dataW * es + 15) & ~15u;
-            work.src0 = pf;
-            work.src1 = work.has1 ? pf + rs : pf;
-            work.src_s = true;
         }
+        const int es = a.d.bits == 16 ? 2 : 1;
+        const uint32_t rs = (a.d.dataW * es + 15) & ~15u;
+        work.s_src0 = smem_u32addr(pf);
+        work.s_src1 = work.has1 ? smem_u32addr(pf + rs) : work.s_src0;
     }
     if (valid) {
 #pragma unroll
@@ -1033,6 +1075,20 @@ static void configure_smem(K kern, size_t bytes, unsigned &mask)
 
 static bool aligned16(const void *p, size_t bytes) { return ((uintptr_t)p % 16 == 0) && bytes % 16 == 0; }
 
+// Warp row-pass variant for a launch (update passes: noout when not the
+// last view; sm when the operand rows are bulk-copied into shared memory).
+template <int W, int MODE, int BITS>
+static void pick_row_w(bool noout, bool sm, void (*&kern)(const RowArgs), unsigned *&m)
+{
+    static unsigned mask[4] = {0, 0, 0, 0};
+    constexpr bool U = MODE == ROW_UPDATE;
+    if (noout)
+        kern = sm ? row_pass_w<W, MODE, BITS, U, true> : row_pass_w<W, MODE, BITS, U, false>;
+    else
+        kern = sm ? row_pass_w<W, MODE, BITS, false, true> : row_pass_w<W, MODE, BITS, false, false>;
+    m = &mask[(noout ? 1 : 0) + (sm ? 2 : 0)];
+}
+
 template <int W, int MODE>
 static void launch_row(const RowArgs &a0, cudaStream_t s)
 {
@@ -1054,20 +1110,20 @@ static void launch_row(const RowArgs &a0, cudaStream_t s)
         a.group_floats = WF::padded_floats + (int)(pf / sizeof(float));
         const size_t smem = sizeof(float) * kRowWarps * G * (size_t)a.group_floats;
         // the element-wise step is compiled for the sample width
-        // compiled per sample width, and for the update pass per last / not last
+        // compiled per sample width, per operand rows in shared memory or
+        // not, and for the update pass per last / not last
         void (*kern)(const RowArgs);
-        static unsigned mask[5] = {0, 0, 0, 0, 0};
         unsigned *m;
         const bool noout = MODE == ROW_UPDATE && !a.last;
+        const bool sm = MODE == ROW_UPDATE ? a.bulk_weights != 0 : (MODE == ROW_DIVIDE && a.bulk_data != 0);
         if constexpr (MODE == ROW_INIT) {
-            kern = row_pass_w<W, MODE, 0, false>;
-            m = &mask[0];
+            static unsigned mask0 = 0;
+            kern = row_pass_w<W, MODE, 0, false, false>;
+            m = &mask0;
         } else if (a.d.bits == 16) {
-            kern = noout ? row_pass_w<W, MODE, 16, MODE == ROW_UPDATE> : row_pass_w<W, MODE, 16, false>;
-            m = &mask[noout ? 3 : 1];
+            pick_row_w<W, MODE, 16>(noout, sm, kern, m);
         } else {
-            kern = noout ? row_pass_w<W, MODE, 8, MODE == ROW_UPDATE> : row_pass_w<W, MODE, 8, false>;
-            m = &mask[noout ? 4 : 2];
+            pick_row_w<W, MODE, 8>(noout, sm, kern, m);
         }
         configure_smem(kern, 200 * 1024, *m);
         dim3 grid((a.d.H + kRowWarps * G - 1) / (kRowWarps * G), a.b.npairs);
