@@ -137,6 +137,8 @@ std::vector<double2> twiddles_d(int n)
 //   [J * T + t] = exp(-2 pi i t / N)
 std::vector<float2> warp_twiddles(int n)
 {
+    if (n > 1024)
+        return warp_twiddles(kLineM);  // lines above 1024 run 512-point sub-transforms
     std::vector<float2> t(rl_warp_twiddle_entries(n), make_float2(0.f, 0.f));
     const int T = rl_warp_lanes(n);
     if (T == 0)

@@ -98,6 +98,7 @@ struct RowArgs {
     int bulk_data;      // data rows may be fetched with 16-byte bulk copies
     int bulk_weights;   // weight rows may be fetched with 16-byte bulk copies
     int group_floats;   // warp engine: shared floats per group (transpose + prefetch)
+    const float2 *twN;  // lines above 1024: exp(-2 pi i n / W), n < W
 };
 
 template <int W, int F>
@@ -577,8 +578,9 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
 struct ColArgs {
     float2 *C;
     const float2 *spec;  // column-pass launch layout
-    const float2 *tw;
+    const float2 *tw;    // warp-FFT twiddles (of kLineM above 1024)
     int H, W;
+    const float2 *twN;   // columns above 1024: exp(-2 pi i n / H), n < H
 };
 
 template <int H, int F>
@@ -860,6 +862,282 @@ __global__ void __launch_bounds__(CW * 32, FMVD_COL_MIN_BLOCKS) col_pass_w(const
     }
 }
 
+// -------------------------------------- lines above 1024: R x 512 engine
+// A line of N = R * kLineM points (R = 3..8, every supported length above
+// 1024) is split over R groups of 16 lanes (half-warps), each running the
+// 512-point warp FFT on one sub-line.  Frequencies R k1 + r live in sub-line
+// r at position k1 (the work planes keep rows in this order between passes,
+// and the column pass's spectrum follows it); space positions n1 + 512 q
+// live in group q:
+//   frequency -> space:  Z_r = FFT512(sub-line r), Z_r[n1] *= w_N^(r n1),
+//                        x[n1 + 512 q] = sum_r Z_r[n1] w_R^(q r)
+//   space -> frequency:  u_r[n1] = sum_q x[n1 + 512 q] w_R^(q r),
+//                        u_r[n1] *= w_N^(r n1), sub-line r = FFT512(u_r)
+// (forward sign; the inverse is conj(forward(conj))).  The sums over the R
+// groups go through shared memory between two block barriers.
+
+// v[m] *= w_N^(r n1), n1 = t + 16 m (twN: w_N^n, n < N): the table value
+// for every eighth m, times powers of w_N^(16 r) in between (at most seven
+// rounding steps; few table addresses live at once)
+__device__ __forceinline__ void line_twiddle(float2 *v, const float2 *__restrict__ twN, int r, int t)
+{
+    const float2 step = __ldg(twN + 16 * r);
+#pragma unroll
+    for (int m0 = 0; m0 < 32; m0 += 8) {
+        float2 w = __ldg(twN + r * (t + 16 * m0));
+#pragma unroll
+        for (int m = m0; m < m0 + 8; m++) {
+            v[m] = cmul(v[m], w);
+            if (m + 1 < m0 + 8)
+                w = cmul(w, step);
+        }
+    }
+}
+
+// w_R^(r j) (twN: w_N^n with N = R * kLineM)
+template <int R>
+__device__ __forceinline__ float2 line_coefficient(const float2 *__restrict__ twN, int r, int j)
+{
+    return __ldg(twN + ((r * j) % R) * kLineM);
+}
+
+// Row pass for W = R * 512: R warps, two rows per block (half-warp h of warp
+// r is group r of row h).
+template <int R, int MODE, int BITS, bool NOOUT>
+__global__ void __launch_bounds__(R * 32, 16 / R) row_pass_r(const RowArgs a)
+{
+    using WF = WarpFft<kLineM>;
+    constexpr int T = WF::T, E = WF::E, PF2 = WF::padded_f2, N = R * kLineM;
+    static_assert(T == 16 && E == 32, "sub-lines are 512-point half-warp transforms");
+    extern __shared__ __align__(16) float smem[];
+    const int r = threadIdx.x >> 5;
+    const int h = (threadIdx.x >> 4) & 1;
+    const int t = threadIdx.x & 15;
+    float2 *const lbuf = reinterpret_cast<float2 *>(smem) + (size_t)h * R * PF2;  // the row's R buffers
+    float2 *const buf = lbuf + (size_t)r * PF2;
+    const int y = blockIdx.x * 2 + h;
+    const int p = blockIdx.y;
+    float2 *row = a.b.C + ((size_t)p * a.d.H + y) * N + r * kLineM;
+    RowWork<MODE, BITS, NOOUT> work(a, p, y);
+
+    // the sum over the row's R groups: v[m] = sum_j (group j's v[m]) w_R^(r j)
+    const auto line_sum = [&](float2 *v) {
+#pragma unroll
+        for (int m = 0; m < E; m++)
+            buf[t + T * m] = v[m];
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < E; m++)
+            v[m] = lbuf[t + T * m];
+#pragma unroll
+        for (int j = 1; j < R; j++) {
+            const float2 cj = line_coefficient<R>(a.twN, r, j);
+#pragma unroll
+            for (int m = 0; m < E; m++)
+                v[m] = cadd(v[m], cmul(lbuf[j * PF2 + t + T * m], cj));
+        }
+        __syncthreads();
+    };
+
+    // pass 0: frequency -> space (the inverse as conj(forward(conj))) and
+    // the element-wise step; pass 1: space -> frequency.  The rolled loop
+    // keeps one copy of the 512-point transform.
+    float2 v[E];
+    if (MODE == ROW_INIT) {
+#pragma unroll
+        for (int m = 0; m < E; m++) {
+            v[m] = make_float2(0.f, 0.f);
+            work.apply(r * kLineM + t + T * m, v[m]);
+        }
+    } else {
+#pragma unroll
+        for (int m = 0; m < E; m++) {
+            const float2 x = row[t + T * m];
+            v[m] = make_float2(x.x, -x.y);
+        }
+    }
+#pragma unroll 1
+    for (int pass = MODE == ROW_INIT ? 1 : 0; pass < 2; pass++) {
+        if (pass == 1) {
+            line_sum(v);
+            line_twiddle(v, a.twN, r, t);
+        }
+        WF::template run_padded<-1>(v, a.tw, buf, t);
+        if (pass == 1)
+            break;
+        line_twiddle(v, a.twN, r, t);
+        line_sum(v);
+#pragma unroll
+        for (int m = 0; m < E; m++) {
+            v[m].y = -v[m].y;
+            work.apply(r * kLineM + t + T * m, v[m]);
+        }
+        if (MODE == ROW_UPDATE && !NOOUT && a.last)
+            return;
+    }
+#pragma unroll
+    for (int m = 0; m < E; m++)
+        row[t + T * m] = v[m];
+}
+
+// Column tile of the line engine: two columns, element (y, c) at float2
+// 2 y + (c ^ ((y >> 3) & 1)): sixteen consecutive rows of one column fall in
+// sixteen distinct 8-byte slots of a 256-byte window.  With the tile on a
+// 256-byte boundary, row y = 512 r + 16 a + u (u < 16) of column c is at
+// byte 8192 r + 256 a + 8 Q_c(u), Q_c(u) = 2 u + (c ^ ((u >> 3) & 1)), and
+// Q_c is XOR-linear: Q_c(t ^ k) = Q_c(t) ^ R16(k), R16(k) = 2 k + ((k >> 3) & 1).
+__device__ __forceinline__ int coltile_r(int y, int c) { return 2 * y + (c ^ ((y >> 3) & 1)); }
+__host__ __device__ constexpr uint32_t coltile16_r(int k) { return 2u * k + ((k >> 3) & 1); }
+
+// 512-point transform (WarpFft<512>: T = 16, E = 32) of one sub-line of a
+// line-engine column tile, its own rows as transpose space:
+// wbase = sub-line start | 8 Q_c(t), rbase = (sub-line start + 256 t) | 8 Q_c(t).
+template <int DIR, typename TW>
+__device__ __forceinline__ void col_fft_512(float2 *v, const TW &tw, uint32_t wbase, uint32_t rbase, int t)
+{
+    using WF = WarpFft<kLineM>;
+    Dft<32, DIR>::run(v);
+    WF::template twiddle<DIR>(v, tw, t);
+#pragma unroll
+    for (int k1 = 0; k1 < 32; k1++)
+        sts2((wbase ^ (8u * coltile16_r(k1 & 15))) + 256u * k1, v[k1]);
+    __syncwarp();
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+#pragma unroll
+        for (int j = 0; j < 16; j++)
+            v[s * 16 + j] = lds2((rbase ^ (8u * coltile16_r(j))) + 4096u * s);
+    __syncwarp();
+    Dft<16, DIR>::run(v);
+    Dft<16, DIR>::run(v + 16);
+    WF::reorder(v);
+}
+
+// Column pass for H = R * 512: R warps, two columns per block (half-warp cc
+// of warp r is group r of column cc).  Spectrum in launch layout: block bx,
+// register m, thread tid at spec[(bx * 32 + m) * (32 R) + tid].
+template <int R>
+__global__ void __launch_bounds__(R * 32, 16 / R) col_pass_r(const ColArgs a)
+{
+    using WF = WarpFft<kLineM>;
+    constexpr int T = WF::T, E = WF::E, H = R * kLineM, NT = R * 32;
+    extern __shared__ __align__(16) float smem[];
+    const uint32_t s0 = smem_u32addr(smem);
+    const uint32_t base = (s0 + 255u) & ~255u;
+    float2 *tile = reinterpret_cast<float2 *>(reinterpret_cast<char *>(smem) + (base - s0));
+    const int W = a.W;
+    const int p = blockIdx.y;
+    float2 *C = a.C + (size_t)p * H * W + 2 * blockIdx.x;
+#pragma unroll 8
+    for (int i = 0; i < 2 * H / NT; i++) {
+        const int u = threadIdx.x + i * NT;
+        const int y = u >> 1, c = u & 1;
+        cp_async8(tile + coltile_r(y, c), C + (size_t)y * W + c);
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    const int r = threadIdx.x >> 5;
+    const int cc = (threadIdx.x >> 4) & 1;
+    const int t = threadIdx.x & 15;
+    const uint32_t q = 8u * (2 * t + (cc ^ ((t >> 3) & 1)));
+    const uint32_t col = base + q;                  // + 8192 j + 256 m: row 512 j + t + 16 m
+    const uint32_t seg = base + 8192u * r;          // this group's sub-line
+    const uint32_t wbase = seg | q, rbase = (seg + 256u * t) | q;
+
+    // v[m] = sum_j (row 512 j + t + 16 m of this column) w_R^(r j)
+    const auto column_sum = [&](float2 *v) {
+#pragma unroll
+        for (int m = 0; m < E; m++)
+            v[m] = lds2(col + 256u * m);
+#pragma unroll
+        for (int j = 1; j < R; j++) {
+            const float2 cj = line_coefficient<R>(a.twN, r, j);
+#pragma unroll
+            for (int m0 = 0; m0 < E; m0 += 8) {
+                asm volatile("" ::: "memory");  // bounds the loads in flight
+#pragma unroll
+                for (int m = m0; m < m0 + 8; m++)
+                    v[m] = cadd(v[m], cmul(lds2(col + 8192u * j + 256u * m), cj));
+            }
+        }
+        asm volatile("" ::: "memory");
+    };
+
+    float2 v[E];
+    // pass 0: space -> frequency, times the spectrum, conjugated; pass 1:
+    // the same forward pipeline then runs frequency -> space.  The rolled
+    // loop keeps one copy of the transform (its table loads are not kept
+    // live from one copy to the next).
+    const float2 *sp = a.spec + (size_t)blockIdx.x * E * NT + threadIdx.x;
+#pragma unroll 1
+    for (int pass = 0; pass < 2; pass++) {
+        if (pass == 0) {
+            column_sum(v);
+            __syncthreads();  // every group has read the column before transposes overwrite it
+            line_twiddle(v, a.twN, r, t);
+        }
+        col_fft_512<-1>(v, a.tw, wbase, rbase, t);
+        if (pass == 1)
+            break;
+#pragma unroll
+        for (int m0 = 0; m0 < E; m0 += 8) {
+            asm volatile("" ::: "memory");
+#pragma unroll
+            for (int m = m0; m < m0 + 8; m++) {
+                const float2 z = cmul(v[m], __ldg(sp + (size_t)m * NT));
+                v[m] = make_float2(z.x, -z.y);
+            }
+        }
+        asm volatile("" ::: "memory");
+    }
+    line_twiddle(v, a.twN, r, t);
+#pragma unroll
+    for (int m = 0; m < E; m++)
+        sts2(seg + q + 256u * m, v[m]);  // row 512 r + t + 16 m
+    __syncthreads();
+    column_sum(v);
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < E; m++)
+        sts2(seg + q + 256u * m, make_float2(v[m].x, -v[m].y));
+    __syncthreads();
+#pragma unroll 4
+    for (int i = 0; i < H / NT; i++) {
+        const int y = threadIdx.x + i * NT;
+        const float2 e0 = tile[coltile_r(y, 0)], e1 = tile[coltile_r(y, 1)];
+        *reinterpret_cast<float4 *>(C + (size_t)y * W) = make_float4(e0.x, e0.y, e1.x, e1.y);
+    }
+}
+
+// Frequency of stored column (or row position) j of a line of length n:
+// natural up to 1024, the R x 512 order above.
+__host__ __device__ __forceinline__ int stored_frequency(int j, int n)
+{
+    if (n <= 1024)
+        return j;
+    const int R = n / kLineM;
+    return R * (j % kLineM) + j / kLineM;
+}
+
+// Launch layout of the line engine's column-pass spectrum: block bx
+// (stored columns 2 bx, 2 bx + 1), register m, thread tid = 32 r + 16 cc + t
+// holds frequency ky = R (t + 16 m) + r of stored column 2 bx + cc.
+__global__ void permute_spectrum_r(const double2 *__restrict__ nat, float2 *__restrict__ out, int H, int W, double scale)
+{
+    const int R = H / kLineM, NT = 32 * R;
+    const size_t total = (size_t)H * W;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int tid = (int)(i % NT);
+        const int m = (int)((i / NT) % 32);
+        const int bx = (int)(i / ((size_t)NT * 32));
+        const int r = tid >> 5, cc = (tid >> 4) & 1, t = tid & 15;
+        const int ky = R * (t + 16 * m) + r;
+        const int kx = stored_frequency(2 * bx + cc, W);
+        const double2 k = nat[(size_t)ky * W + kx];
+        out[i] = make_float2((float)(k.x * scale), (float)(k.y * scale));
+    }
+}
+
 // Launch layout of the column-pass spectrum for the warp engine.
 __global__ void permute_spectrum_w(const double2 *__restrict__ nat, float2 *__restrict__ out, int H, int W, int T,
                                    int CW, double scale)
@@ -873,7 +1151,7 @@ __global__ void permute_spectrum_w(const double2 *__restrict__ nat, float2 *__re
         const int warp = tid >> 5, lane = tid & 31;
         const int g = lane / T, t = lane % T;
         const int n = t + T * m;
-        const int col = bx * FC + warp * G + g;
+        const int col = stored_frequency(bx * FC + warp * G + g, W);
         const double2 k = nat[(size_t)n * W + col];
         out[i] = make_float2((float)(k.x * scale), (float)(k.y * scale));
     }
@@ -1040,14 +1318,7 @@ int rl_col_warps(int H, int W, int requested)
     return ok ? requested : -1;
 }
 
-size_t rl_spectrum_elems(int H, int W)
-{
-    if (H <= 1024)
-        return (size_t)H * W;
-    const int F = col_f(H);
-    const int NT = F * H / kE;
-    return (size_t)(W / F) * kE * NT;
-}
+size_t rl_spectrum_elems(int H, int W) { return (size_t)H * W; }
 
 void rl_upload_constants()
 {
@@ -1087,6 +1358,26 @@ static void pick_row_w(bool noout, bool sm, void (*&kern)(const RowArgs), unsign
     else
         kern = sm ? row_pass_w<W, MODE, BITS, false, true> : row_pass_w<W, MODE, BITS, false, false>;
     m = &mask[(noout ? 1 : 0) + (sm ? 2 : 0)];
+}
+
+// Line-engine row-pass variant for a launch (per sample width; update
+// passes per last / not last).
+template <int R, int MODE>
+static void pick_row_r(const RowArgs &a, void (*&kern)(const RowArgs), unsigned *&m)
+{
+    static unsigned mask[5] = {0, 0, 0, 0, 0};
+    const bool noout = MODE == ROW_UPDATE && !a.last;
+    constexpr bool U = MODE == ROW_UPDATE;
+    if constexpr (MODE == ROW_INIT) {
+        kern = row_pass_r<R, MODE, 0, false>;
+        m = &mask[0];
+    } else if (a.d.bits == 16) {
+        kern = noout ? row_pass_r<R, MODE, 16, U> : row_pass_r<R, MODE, 16, false>;
+        m = &mask[noout ? 3 : 1];
+    } else {
+        kern = noout ? row_pass_r<R, MODE, 8, U> : row_pass_r<R, MODE, 8, false>;
+        m = &mask[noout ? 4 : 2];
+    }
 }
 
 template <int W, int MODE>
@@ -1129,36 +1420,15 @@ static void launch_row(const RowArgs &a0, cudaStream_t s)
         dim3 grid((a.d.H + kRowWarps * G - 1) / (kRowWarps * G), a.b.npairs);
         kern<<<grid, kRowWarps * 32, smem, s>>>(a);
     } else {
-        constexpr int F = row_f(W);
-        using PF = BlockRowPrefetch<W, F>;
-        RowArgs a = a0;
-        const size_t es = a.d.bits == 16 ? 2 : 1;
-        a.bulk_data = aligned16(a.b.data, a.d.dataW * es) && (a.b.view_stride * es) % 16 == 0 &&
-                      (a.b.plane_stride * es) % 16 == 0;
-        a.bulk_weights = aligned16(a.b.weights, a.d.dataW * sizeof(float)) &&
-                         ((size_t)a.d.dataH * a.d.dataW * sizeof(float)) % 16 == 0;
-        size_t pf = 0;
-        if (MODE == ROW_UPDATE)
-            pf = F * W * sizeof(float2) + (a.bulk_weights ? F * PF::row_bytes(a.d.dataW * sizeof(float)) : 0);
-        else if (MODE == ROW_DIVIDE && a.bulk_data)
-            pf = 2 * F * PF::row_bytes(a.d.dataW * es);
-        const size_t smem = PF::offset + pf;
+        constexpr int R = W / kLineM;
+        static_assert(W % kLineM == 0 && R >= 3 && R <= 8, "rows above 1024 are 3..8 sub-lines of 512");
+        const size_t smem = sizeof(float2) * 2 * R * WarpFft<kLineM>::padded_f2;
         void (*kern)(const RowArgs);
-        static unsigned mask[3] = {0, 0, 0};
         unsigned *m;
-        if constexpr (MODE == ROW_INIT) {
-            kern = row_pass<W, F, MODE, 0>;
-            m = &mask[0];
-        } else if (a.d.bits == 16) {
-            kern = row_pass<W, F, MODE, 16>;
-            m = &mask[1];
-        } else {
-            kern = row_pass<W, F, MODE, 8>;
-            m = &mask[2];
-        }
-        configure_smem(kern, 200 * 1024, *m);
-        dim3 grid(a.d.H / F, a.b.npairs);
-        kern<<<grid, Cfg<W, F>::NT, smem, s>>>(a);
+        pick_row_r<R, MODE>(a0, kern, m);
+        configure_smem(kern, smem, *m);
+        dim3 grid(a0.d.H / 2, a0.b.npairs);
+        kern<<<grid, R * 32, smem, s>>>(a0);
     }
     g_launches++;
 }
@@ -1187,13 +1457,14 @@ static void launch_col(const ColArgs &a, int npairs, int cw, cudaStream_t s)
         default: launch_col_w<H, 2>(a, npairs, s); break;
         }
     } else {
-        constexpr int F = col_f(H);
-        using C = Cfg<H, F>;
-        auto kern = col_pass<H, F>;
+        constexpr int R = H / kLineM;
+        static_assert(H % kLineM == 0 && R >= 3 && R <= 8, "columns above 1024 are 3..8 sub-lines of 512");
+        constexpr size_t smem = sizeof(float2) * 2 * H + 256;  // tile aligned to 256 bytes in the kernel
+        auto kern = col_pass_r<R>;
         static unsigned mask = 0;
-        configure_smem(kern, C::smem, mask);
-        dim3 grid(a.W / F, npairs);
-        kern<<<grid, C::NT, C::smem, s>>>(a);
+        configure_smem(kern, smem, mask);
+        dim3 grid(a.W / 2, npairs);
+        kern<<<grid, R * 32, smem, s>>>(a);
     }
     g_launches++;
 }
@@ -1210,29 +1481,27 @@ static void dispatch_row(const RowArgs &a, cudaStream_t s)
     }
 }
 
-static const float2 *row_table(const RlDims &d, const RlTables &t) { return d.W <= 1024 ? t.wtwW : t.twW; }
-
 void rl_init(const RlDims &d, const RlBatch &b, const RlTables &t, cudaStream_t s)
 {
-    RowArgs a{d, b, row_table(d, t), 0, 0, 0, 0, 0};
+    RowArgs a{d, b, t.wtwW, 0, 0, 0, 0, 0, t.twW};
     dispatch_row<ROW_INIT>(a, s);
 }
 
 void rl_divide(const RlDims &d, const RlBatch &b, const RlTables &t, int view, cudaStream_t s)
 {
-    RowArgs a{d, b, row_table(d, t), view, 0, 0, 0, 0};
+    RowArgs a{d, b, t.wtwW, view, 0, 0, 0, 0, t.twW};
     dispatch_row<ROW_DIVIDE>(a, s);
 }
 
 void rl_update(const RlDims &d, const RlBatch &b, const RlTables &t, int view, bool last, cudaStream_t s)
 {
-    RowArgs a{d, b, row_table(d, t), view, last ? 1 : 0, 0, 0, 0};
+    RowArgs a{d, b, t.wtwW, view, last ? 1 : 0, 0, 0, 0, t.twW};
     dispatch_row<ROW_UPDATE>(a, s);
 }
 
 void rl_col(const RlDims &d, const RlBatch &b, const RlTables &t, const float2 *spectrum, cudaStream_t s)
 {
-    ColArgs a{b.C, spectrum, d.H <= 1024 ? t.wtwH : t.twH, d.H, d.W};
+    ColArgs a{b.C, spectrum, t.wtwH, d.H, d.W, t.twH};
     switch (d.H) {
 #define X(N) \
     case N: launch_col<N>(a, b.npairs, d.col_warps ? d.col_warps : col_warps(d.H, d.W), s); break;
@@ -1246,6 +1515,8 @@ int rl_warp_lanes(int n) { return n <= 1024 ? warp_fft_lanes(n) : 0; }
 
 int rl_warp_twiddle_entries(int n)
 {
+    if (n > 1024)
+        return rl_warp_twiddle_entries(kLineM);
     const int T = rl_warp_lanes(n);
     if (T == 0)
         return n;
@@ -1268,8 +1539,7 @@ void rl_kernel_spectrum(const float *d_kernel, int kH, int kW, int H, int W, con
         permute_spectrum_w<<<blocks, 256, 0, s>>>(K, d_out, H, W, warp_fft_lanes(H), cw ? cw : col_warps(H, W),
                                                   scale);
     } else {
-        const int F = col_f(H);
-        permute_spectrum<<<blocks, 256, 0, s>>>(K, d_out, H, W, F, F * H / kE, sched_edge(H), scale);
+        permute_spectrum_r<<<blocks, 256, 0, s>>>(K, d_out, H, W, scale);
     }
 }
 

@@ -41,12 +41,15 @@ struct RlBatch {
 struct RlTables {
     const float2 *twH;   // exp(-2 pi i n / H)            (lengths above 1024)
     const float2 *twW;   // exp(-2 pi i n / W)
-    const float2 *wtwH;  // warp-FFT twiddles of H (lengths <= 1024; layout in warp_twiddles)
+    const float2 *wtwH;  // warp-FFT twiddles of H (of kLineM above 1024; layout in warp_twiddles)
     const float2 *wtwW;  // warp-FFT twiddles of W
 };
 
 // Lanes per line of the warp FFT for length n (0 when n > 1024).
 int rl_warp_lanes(int n);
+// Lines longer than 1024 (R x kLineM, R = 3..8) are split into R sub-lines
+// of this length.
+constexpr int kLineM = 512;
 // Twiddle run of the warp FFT: lane t forms w_N^(t k1), k1 = R j + b, as the
 // table entry w_N^(R j t) times (w_N^t)^b, b < R (R = min(E, this)).
 constexpr int kWarpTwiddleRun = 2;
