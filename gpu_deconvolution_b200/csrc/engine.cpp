@@ -158,8 +158,6 @@ std::vector<float2> warp_twiddles(int n)
     return t;
 }
 
-unsigned g_constants_uploaded = 0;
-
 } // namespace
 
 int default_pairs_cap(int H, int W, int lanes)
@@ -205,12 +203,6 @@ Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weig
     int dev = 0;
     if (!FMVD_CHECK(cudaGetDevice(&dev)))
         return nullptr;
-    if (!(g_constants_uploaded & (1u << (dev & 31)))) {
-        rl_upload_constants();
-        if (!FMVD_CHECK(cudaGetLastError()))
-            return nullptr;
-        g_constants_uploaded |= 1u << (dev & 31);
-    }
 
     Engine *e = new Engine();
     memset(e, 0, sizeof(Engine));

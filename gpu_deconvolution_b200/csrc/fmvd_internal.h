@@ -33,7 +33,7 @@ struct Engine {
     float *weights;         // V x dataH x dataW normalised weights
     float2 *C;              // pairs_cap x H x W
     float2 *est;            // pairs_cap x H x W
-    float2 *twH, *twW;      // exp(-2 pi i n / N), block engine
+    float2 *twH, *twW;      // exp(-2 pi i n / N), line engine (lengths above 1024)
     float2 *wtwH, *wtwW;    // warp engine twiddle tables
     int *status;            // device flag: a bulk-copy wait timed out
     // Second lane: alternate batches run on a side stream with their own

@@ -75,17 +75,6 @@ __device__ __forceinline__ float lds_sample(uint32_t row, int sx)
     return (float)v;
 }
 
-// Rows per row-pass block and columns per column-pass block.
-__host__ __device__ constexpr int row_f(int W) { return W <= 1024 ? 2048 / W : 2; }
-__host__ __device__ constexpr int col_f(int H) { return H <= 256 ? 2048 / H : (H <= 1024 ? 8 : 4); }
-constexpr int kE = 16;  // complex values per thread
-
-template <int N, int F>
-struct Cfg {
-    static constexpr int NT = F * N / kE;
-    static constexpr size_t smem = 2 * sizeof(float) * SmemLayout<N>::floats(F);
-};
-
 // ----------------------------------------------------------- row passes
 enum RowMode { ROW_INIT = 0, ROW_DIVIDE = 1, ROW_UPDATE = 2 };
 
@@ -100,43 +89,6 @@ struct RowArgs {
     int group_floats;   // warp engine: shared floats per group (transpose + prefetch)
     const float2 *twN;  // lines above 1024: exp(-2 pi i n / W), n < W
 };
-
-template <int W, int F>
-__device__ __forceinline__ void load_rows(const float2 *__restrict__ src, float *sre, float *sim)
-{
-    using L = SmemLayout<W>;
-    constexpr int NT = Cfg<W, F>::NT;
-    constexpr int units = F * W / 2;  // float4 = two complex
-    const float4 *s4 = reinterpret_cast<const float4 *>(src);
-#pragma unroll 4
-    for (int u = threadIdx.x; u < units; u += NT) {
-        const int l = 2 * u;
-        const int yl = l / W, x = l % W;
-        const float4 q = s4[u];
-        const int a = L::at(yl, x);
-        sre[a] = q.x;
-        sim[a] = q.y;
-        const int a1 = L::at(yl, x + 1);
-        sre[a1] = q.z;
-        sim[a1] = q.w;
-    }
-}
-
-template <int W, int F>
-__device__ __forceinline__ void store_rows(float2 *__restrict__ dst, const float *sre, const float *sim)
-{
-    using L = SmemLayout<W>;
-    constexpr int NT = Cfg<W, F>::NT;
-    constexpr int units = F * W / 2;
-    float4 *d4 = reinterpret_cast<float4 *>(dst);
-#pragma unroll 4
-    for (int u = threadIdx.x; u < units; u += NT) {
-        const int l = 2 * u;
-        const int yl = l / W, x = l % W;
-        const int a = L::at(yl, x), a1 = L::at(yl, x + 1);
-        d4[u] = make_float4(sre[a], sim[a], sre[a1], sim[a1]);
-    }
-}
 
 // Sample loads and estimate traffic are streamed (evict-first in L2) so that
 // the batch's complex work planes stay resident in L2 between passes.
@@ -283,128 +235,6 @@ struct RowWork {
         }
     }
 };
-
-template <int MODE, int BITS>
-__device__ __forceinline__ void pointwise(const RowArgs &a, int p, int y, int x, float2 &v)
-{
-    RowWork<MODE, BITS>(a, p, y).apply(x, v);
-}
-
-// Row pass for W > 1024: F rows per block through the shared-memory Stockham engine.
-// Blocks per SM the register allocation of the block-engine passes must allow.
-#ifndef FMVD_BLOCK_ROW_MIN_BLOCKS
-#define FMVD_BLOCK_ROW_MIN_BLOCKS 1
-#endif
-#ifndef FMVD_BLOCK_COL_MIN_BLOCKS
-#define FMVD_BLOCK_COL_MIN_BLOCKS 1
-#endif
-// Shared-memory prefetch of the element-wise operand rows of a block-engine
-// row pass: bytes after the transform arrays.
-template <int W, int F>
-struct BlockRowPrefetch {
-    static constexpr size_t offset = (Cfg<W, F>::smem + 15) & ~(size_t)15;
-    static __host__ __device__ size_t row_bytes(size_t b) { return (b + 15) & ~(size_t)15; }
-};
-
-template <int W, int F, int MODE, int BITS>
-__global__ void __launch_bounds__(Cfg<W, F>::NT, FMVD_BLOCK_ROW_MIN_BLOCKS) row_pass(const RowArgs a)
-{
-    extern __shared__ __align__(16) float smem[];
-    __shared__ __align__(8) uint64_t pbar;
-    float *sre = smem;
-    float *sim = smem + SmemLayout<W>::floats(F);
-    constexpr int NT = Cfg<W, F>::NT;
-    using EG = Edge<W, F, NT>;
-    using PF = BlockRowPrefetch<W, F>;
-    const int p = blockIdx.y;
-    const int y0 = blockIdx.x * F;
-    float2 *C = a.b.C + (size_t)p * a.d.H * W + (size_t)y0 * W;
-    float2 v[EG::E];
-
-    // The estimate and weight rows (update) or the data rows (divide) of the
-    // block's F rows arrive by bulk copy while the inverse transform runs.
-    char *pf = reinterpret_cast<char *>(smem) + PF::offset;
-    const int es = a.d.bits == 16 ? 2 : 1;
-    const bool has1 = 2 * p + 1 < a.b.nplanes;
-    const size_t wrb = PF::row_bytes((size_t)a.d.dataW * sizeof(float));
-    const size_t drb = PF::row_bytes((size_t)a.d.dataW * es);
-    const bool prefetch = (MODE == ROW_UPDATE) || (MODE == ROW_DIVIDE && a.bulk_data);
-    if (prefetch && threadIdx.x == 0) {
-        mbar_init(&pbar, 1);
-        mbar_fence_init();
-        if (MODE == ROW_UPDATE) {
-            const uint32_t eb = F * W * sizeof(float2);
-            const uint32_t wb = a.bulk_weights ? F * (uint32_t)a.d.dataW * sizeof(float) : 0;
-            mbar_arrive_expect_tx(&pbar, eb + wb);
-            bulk_load(pf, a.b.est + ((size_t)p * a.d.H + y0) * W, eb, &pbar);
-            if (a.bulk_weights)
-                for (int f = 0; f < F; f++)
-                    bulk_load(pf + eb + f * wrb,
-                              a.b.weights + (size_t)a.view * a.d.dataH * a.d.dataW +
-                                  (size_t)clamp_src(y0 + f, a.d.dataH, a.d.byW) * a.d.dataW,
-                              a.d.dataW * sizeof(float), &pbar);
-        } else {
-            const uint32_t rb = a.d.dataW * es;
-            mbar_arrive_expect_tx(&pbar, F * rb * (has1 ? 2 : 1));
-            for (int f = 0; f < F; f++) {
-                const size_t base = (size_t)a.view * a.b.view_stride +
-                                    (size_t)clamp_src(y0 + f, a.d.dataH, a.d.byD) * a.d.dataW;
-                bulk_load(pf + (2 * f) * drb, (const char *)a.b.data + (base + (size_t)(2 * p) * a.b.plane_stride) * es,
-                          rb, &pbar);
-                if (has1)
-                    bulk_load(pf + (2 * f + 1) * drb,
-                              (const char *)a.b.data + (base + (size_t)(2 * p + 1) * a.b.plane_stride) * es, rb, &pbar);
-            }
-        }
-    }
-
-    if (MODE != ROW_INIT) {
-        load_rows<W, F>(C, sre, sim);
-        __syncthreads();
-        fft<W, F, NT, +1, false>(sre, sim, v, a.tw);
-    }
-    {
-        // the element-wise state of this thread's first row, built once (a
-        // thread's slots usually all lie in one row)
-        int f0, x0;
-        EG::pos(0, f0, x0);
-        RowWork<MODE, BITS> w0(a, p, y0 + f0);
-        if (prefetch) {
-            if (!mbar_wait(&pbar, 0)) {
-                // the copies did not land in time: flag it, wait once more so
-                // none is left in flight, and read from global memory
-                if (threadIdx.x == 0)
-                    atomicExch(a.b.status, 1);
-                mbar_wait(&pbar, 0);
-            } else if (MODE == ROW_UPDATE) {
-                w0.est_s = reinterpret_cast<const float2 *>(pf) + (size_t)f0 * W;
-                if (a.bulk_weights) {
-                    w0.wrow = reinterpret_cast<const float *>(pf + F * W * sizeof(float2) + f0 * wrb);
-                    w0.w_s = true;
-                }
-            } else {
-                w0.src0 = pf + (2 * f0) * drb;
-                w0.src1 = has1 ? pf + (2 * f0 + 1) * drb : w0.src0;
-                w0.src_s = true;
-            }
-        }
-#pragma unroll
-        for (int e = 0; e < EG::E; e++) {
-            int f, x;
-            EG::pos(e, f, x);
-            if (f == f0)
-                w0.apply(x, v[e]);
-            else
-                pointwise<MODE, BITS>(a, p, y0 + f, x, v[e]);
-        }
-    }
-    if (MODE == ROW_UPDATE && a.last)
-        return;
-    fft<W, F, NT, -1, true>(sre, sim, v, a.tw);
-    regs_to_smem<W, F, NT>(sre, sim, v);
-    __syncthreads();
-    store_rows<W, F>(C, sre, sim);
-}
 
 // Row pass for W <= 1024: one group of T lanes per row, warp FFT, no block
 // synchronisation.  Rows beyond H (only for tiny planes) compute on row H-1
@@ -582,53 +412,6 @@ struct ColArgs {
     int H, W;
     const float2 *twN;   // columns above 1024: exp(-2 pi i n / H), n < H
 };
-
-template <int H, int F>
-__global__ void __launch_bounds__(Cfg<H, F>::NT, FMVD_BLOCK_COL_MIN_BLOCKS) col_pass(const ColArgs a)
-{
-    extern __shared__ float smem[];
-    float *sre = smem;
-    float *sim = smem + SmemLayout<H>::floats(F);
-    constexpr int NT = Cfg<H, F>::NT;
-    using EG = Edge<H, F, NT>;
-    using L = SmemLayout<H>;
-    const int W = a.W;
-    const int p = blockIdx.y;
-    const int x0 = blockIdx.x * F;
-    float2 *C = a.C + (size_t)p * H * W;
-
-    // load F columns: units of two complex along x
-    constexpr int units = H * F / 2;
-#pragma unroll 4
-    for (int u = threadIdx.x; u < units; u += NT) {
-        const int c2 = u % (F / 2), y = u / (F / 2);
-        const int x = x0 + 2 * c2;
-        const float4 q = *reinterpret_cast<const float4 *>(C + tile_index(y, x, W));
-        const int a0 = L::at(2 * c2, y), a1 = L::at(2 * c2 + 1, y);
-        sre[a0] = q.x;
-        sim[a0] = q.y;
-        sre[a1] = q.z;
-        sim[a1] = q.w;
-    }
-    __syncthreads();
-
-    float2 v[EG::E];
-    fft<H, F, NT, -1, false>(sre, sim, v, a.tw);
-    const float2 *sp = a.spec + (size_t)blockIdx.x * EG::E * NT + threadIdx.x;
-#pragma unroll
-    for (int e = 0; e < EG::E; e++)
-        v[e] = cmul(v[e], __ldg(sp + (size_t)e * NT));
-    fft<H, F, NT, +1, true>(sre, sim, v, a.tw);
-    regs_to_smem<H, F, NT>(sre, sim, v);
-    __syncthreads();
-#pragma unroll 4
-    for (int u = threadIdx.x; u < units; u += NT) {
-        const int c2 = u % (F / 2), y = u / (F / 2);
-        const int x = x0 + 2 * c2;
-        const int a0 = L::at(2 * c2, y), a1 = L::at(2 * c2 + 1, y);
-        *reinterpret_cast<float4 *>(C + tile_index(y, x, W)) = make_float4(sre[a0], sim[a0], sre[a1], sim[a1]);
-    }
-}
 
 __global__ void write_estimate_kernel(const RlDims d, const RlBatch b)
 {
@@ -1020,7 +803,8 @@ template <int R>
 __global__ void __launch_bounds__(R * 32, 16 / R) col_pass_r(const ColArgs a)
 {
     using WF = WarpFft<kLineM>;
-    constexpr int T = WF::T, E = WF::E, H = R * kLineM, NT = R * 32;
+    static_assert(WF::T == 16 && WF::E == 32, "sub-lines are 512-point half-warp transforms");
+    constexpr int E = WF::E, H = R * kLineM, NT = R * 32;
     extern __shared__ __align__(16) float smem[];
     const uint32_t s0 = smem_u32addr(smem);
     const uint32_t base = (s0 + 255u) & ~255u;
@@ -1157,25 +941,6 @@ __global__ void permute_spectrum_w(const double2 *__restrict__ nat, float2 *__re
     }
 }
 
-// Column-pass launch layout of a natural-order H x W spectrum: block bx,
-// register slot e, thread t -> (row, column) of the edge pattern.
-__global__ void permute_spectrum(const double2 *__restrict__ nat, float2 *__restrict__ out, int H, int W, int F,
-                                 int NT, int R, double scale)
-{
-    const int E = kE;
-    const size_t total = (size_t)(W / F) * E * NT;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-        const int t = (int)(i % NT);
-        const int e = (int)((i / NT) % E);
-        const int bx = (int)(i / ((size_t)NT * E));
-        const int b = e / R, m = e % R;
-        const int q = t + b * NT;
-        const int f = q / (H / R);
-        const int n = q % (H / R) + m * (H / R);
-        const double2 k = nat[(size_t)n * W + (size_t)bx * F + f];
-        out[i] = make_float2((float)(k.x * scale), (float)(k.y * scale));
-    }
-}
 
 // Separable direct DFT of a small kernel placed at (y - kH/2, x - kW/2) mod (H, W).
 // Step 1: A[y][v] = sum_x k[y][x] exp(-2 pi i v (x - cx) / W)
@@ -1293,7 +1058,6 @@ int snap_transform_size(int n)
     return align(n, 512);
 }
 
-static int sched_edge(int n) { return make_schedule(n).r[0]; }
 
 // Warps per column block of the warp engine: the largest of 8, 4, 2 whose
 // columns per block divide W.
@@ -1309,7 +1073,7 @@ static int col_warps(int H, int W)
 int rl_col_warps(int H, int W, int requested)
 {
     if (H > 1024)
-        return 0;  // block engine: fixed column tile
+        return 0;  // line engine: fixed two-column tile
     if (requested == 0)
         return col_warps(H, W);
     const int G = 32 / warp_fft_lanes(H);
@@ -1319,17 +1083,6 @@ int rl_col_warps(int H, int W, int requested)
 }
 
 size_t rl_spectrum_elems(int H, int W) { return (size_t)H * W; }
-
-void rl_upload_constants()
-{
-    static OddRadixTable t;
-    for (int R = 3; R < 32; R += 2)
-        for (int k = 0; k < R; k++) {
-            t.c[R][k] = (float)cos(2.0 * M_PI * k / R);
-            t.s[R][k] = (float)sin(2.0 * M_PI * k / R);
-        }
-    cudaMemcpyToSymbol(g_odd, &t, sizeof(t));
-}
 
 // Dynamic shared memory above 48 KB needs an opt-in per function and device.
 template <typename K>

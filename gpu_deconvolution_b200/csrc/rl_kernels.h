@@ -66,7 +66,6 @@ void rl_count_launch(unsigned long long n);
 // Number of complex values of a column-pass kernel spectrum in its launch layout.
 size_t rl_spectrum_elems(int H, int W);
 
-void rl_upload_constants();  // per device, before the first launch
 void rl_init(const RlDims &d, const RlBatch &b, const RlTables &t, cudaStream_t s);
 void rl_col(const RlDims &d, const RlBatch &b, const RlTables &t, const float2 *spectrum, cudaStream_t s);
 void rl_divide(const RlDims &d, const RlBatch &b, const RlTables &t, int view, cudaStream_t s);

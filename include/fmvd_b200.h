@@ -31,8 +31,8 @@ int fmvd_b200_plan_query(const fmvd_b200_plan *plan, int *fftH, int *fftW, int *
 fmvd_b200_plan *fmvd_b200_plan_create_tuned(int bits, int dataH, int dataW, const float *const *h_Weights,
                                             float **h_Kernel, int kernelH, int kernelW, fmvd_psf_type iteration_type,
                                             int nViews, int pairs_per_batch, int col_warps);
-/* Column-pass warps per block of the plan (0 for the block engine of planes
- * above 1024 rows). */
+/* Column-pass warps per block of the plan (0 for planes above 1024 rows,
+ * whose column pass has a fixed two-column tile). */
 int fmvd_b200_plan_col_warps(const fmvd_b200_plan *plan);
 /* View v, plane z at d_views + (v * view_stride + z * dataH * dataW) samples;
  * output plane z at d_out + z * dataH * dataW.  d_estimate (optional)
