@@ -62,8 +62,12 @@ def parse():
     p.add_argument("--small", action="store_true", help="small volume for profiler captures")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--workload", default="transform_rl", choices=["transform_rl", "warmstart", "batched"],
-                   help="warmstart: learned warm start vs plain RL-50 (time to the RL-50 result)")
+    p.add_argument("--workload", default="transform_rl", choices=["transform_rl", "warmstart", "batched", "planes"],
+                   help="warmstart: learned warm start vs plain RL-50 (time to the RL-50 result); planes: plain "
+                        "RL throughput per padded plane size (--planes)")
+    p.add_argument("--planes", default="1536,2560",
+                   help="planes workload: comma-separated data plane sizes, each padded by a 31 x 31 kernel "
+                        "(63 x 63 above 2000): 1400 -> 1536, 2300 -> 2560")
     p.add_argument("--train-planes", type=int, default=4000)
     p.add_argument("--epochs", type=int, default=12)
     p.add_argument("--target-iterations", type=int, default=42,
@@ -592,6 +596,48 @@ def run_batched(args):
                                "kernels 9..41, 25 iterations)"}}), flush=True)
 
 
+def run_planes(args):
+    """Plain RL on square planes of the given data sizes (4 views, 10
+    iterations, synthetic uint16 views), one JSON line per size: padded
+    voxel-view-iterations per second (padded plane x planes x views x
+    iterations over the CUDA-event time of DevicePlan.run)."""
+    import torch
+    import numpy as np
+    from gpu_deconvolution_b200 import api, synth
+    V, IT = 4, 2 if args.small else 10
+    for size in [int(x) for x in args.planes.split(",") if x]:
+        k = 63 if size > 2000 else 31
+        psfs = [synth.gaussian_psf(k, k, 1.2, 5.0, 45.0 * v) for v in range(V)]
+        weights = [np.ones((size, size), np.float32) for _ in range(V)]
+        plan = api.DevicePlan(size, size, weights, [q.copy() for q in psfs], 0)
+        fh, fw = plan.fftH, plan.fftW
+        D = 8 if args.small else max(8, 2 * int(96e6 // (fh * fw * 8)) * 2)
+        g = torch.Generator(device="cuda").manual_seed(size)
+        views = torch.randint(100, 3000, (V, D, size, size), dtype=torch.int32, device="cuda", generator=g)
+        views = views.to(torch.int16)
+        out = torch.zeros((D, size, size), dtype=torch.int16, device="cuda")
+        for _ in range(max(1, args.warmup)):
+            plan.run(views, out, IT)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(max(1, args.steps)):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            plan.run(views, out, IT)
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        ms = float(np.median(ts))
+        print(json.dumps({"metric": "padded voxel-view-iter/s", "value": fh * fw * D * V * IT / (ms * 1e-3),
+                          "unit": "voxel-view-iter/s", "ms": ms, "higher_is_better": True, "dtype": "f32",
+                          "data": "synthetic",
+                          "config": {"workload": f"plain RL, {V} views, {IT} iterations, {D} planes of "
+                                                 f"{size} x {size} ({k} x {k} PSFs)", "fft_plane": [fh, fw],
+                                     "pairs_per_batch": plan.pairs_per_batch}}), flush=True)
+        plan.destroy()
+        del views, out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -600,6 +646,8 @@ def main():
         run_warmstart(args)
     elif args.workload == "batched":
         run_batched(args)
+    elif args.workload == "planes":
+        run_planes(args)
     else:
         run_b200(args)
 
