@@ -68,6 +68,8 @@ def parse():
     p.add_argument("--planes", default="1536,2560",
                    help="planes workload: comma-separated data plane sizes, each padded by a 31 x 31 kernel "
                         "(63 x 63 above 2000): 1400 -> 1536, 2300 -> 2560")
+    p.add_argument("--pairs-per-batch", type=int, default=0,
+                   help="planes workload: plane pairs per batch (0: the library's default)")
     p.add_argument("--train-planes", type=int, default=4000)
     p.add_argument("--epochs", type=int, default=12)
     p.add_argument("--target-iterations", type=int, default=42,
@@ -609,7 +611,8 @@ def run_planes(args):
         k = 63 if size > 2000 else 31
         psfs = [synth.gaussian_psf(k, k, 1.2, 5.0, 45.0 * v) for v in range(V)]
         weights = [np.ones((size, size), np.float32) for _ in range(V)]
-        plan = api.DevicePlan(size, size, weights, [q.copy() for q in psfs], 0)
+        plan = api.DevicePlan(size, size, weights, [q.copy() for q in psfs], 0,
+                              pairs_per_batch=args.pairs_per_batch)
         fh, fw = plan.fftH, plan.fftW
         D = 8 if args.small else max(8, 2 * int(96e6 // (fh * fw * 8)) * 2)
         g = torch.Generator(device="cuda").manual_seed(size)

@@ -107,6 +107,23 @@ def test_every_fft_length(fh, fw):
     check_outputs(out, oout)
 
 
+@pytest.mark.parametrize("fh,fw", [(1536, 64), (64, 2560)])
+def test_line_engine_8bit_two_views(fh, fw):
+    """8-bit samples, two views with uneven weights and an odd number of
+    planes, on the line engine (rows or columns above 1024)."""
+    k = 7
+    H, W = fh - k + 1, fw - k + 1
+    rng = np.random.default_rng(fh + 3 * fw)
+    views = rng.integers(5, 250, (2, 3, H, W)).astype(np.uint8)
+    psf = [synth.gaussian_psf(k, k, 1.0, 2.0, 30.0 * v) for v in range(2)]
+    w = [rng.uniform(0.3, 1.7, (H, W)).astype(np.float32) for _ in range(2)]
+    out, est = device_estimates(views, w, psf, 0, 2)
+    assert est.shape[1:] == (fh, fw)
+    oout, oest = oracle_estimates(views, w, psf, 0, 2)
+    assert rel_l2(est, oest) < TOL
+    check_outputs(out, oout)
+
+
 def test_config_plane_512_vs_oracle():
     """The plain-RL workload's plane geometry (256^2 data, 17^2 kernels -> 512^2)."""
     views, psfs, weights, _ = synth.plain_rl_views(shape=(2, 256, 256), n_views=2, n_beads=40, ksize=17, seed=8)
