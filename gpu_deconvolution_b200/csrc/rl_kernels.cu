@@ -708,18 +708,6 @@ __global__ void __launch_bounds__(R * 32, 16 / R) row_pass_r(const RowArgs a)
     const int p = blockIdx.y;
     float2 *row = a.b.C + ((size_t)p * a.d.H + y) * N + r * kLineM;
     RowWork<MODE, BITS, NOOUT> work(a, p, y);
-    // the operand rows of this group's space block (positions r * 512 ..
-    // r * 512 + 511) are requested into L1 now and read after the inverse
-    // transform
-    if (MODE == ROW_UPDATE) {
-        prefetch_l1(work.est + r * kLineM + 16 * t);
-        prefetch_l1(work.est + r * kLineM + 16 * (t + 16));
-        prefetch_l1(work.wrow + clamp_src(r * kLineM + 32 * t, a.d.dataW, a.d.bxW));
-    } else if (MODE == ROW_DIVIDE) {
-        const int sx = clamp_src(r * kLineM + 64 * (t & 7), a.d.dataW, a.d.bxD);
-        prefetch_l1((const char *)(t < 8 ? work.src0 : work.src1) + (size_t)sx * (BITS == 8 ? 1 : 2));
-    }
-
     // the sum over the row's R groups: v[m] = sum_j (group j's v[m]) w_R^(r j)
     const auto line_sum = [&](float2 *v) {
 #pragma unroll
@@ -765,6 +753,16 @@ __global__ void __launch_bounds__(R * 32, 16 / R) row_pass_r(const RowArgs a)
         WF::template run_padded<-1>(v, a.tw, buf, t);
         if (pass == 1)
             break;
+        // the operand rows of this group's space block (positions r * 512 ..
+        // r * 512 + 511) are requested into L1 here and read after the sum
+        if (MODE == ROW_UPDATE) {
+            prefetch_l1(work.est + r * kLineM + 16 * t);
+            prefetch_l1(work.est + r * kLineM + 16 * (t + 16));
+            prefetch_l1(work.wrow + clamp_src(r * kLineM + 32 * t, a.d.dataW, a.d.bxW));
+        } else if (MODE == ROW_DIVIDE) {
+            const int sx = clamp_src(r * kLineM + 64 * (t & 7), a.d.dataW, a.d.bxD);
+            prefetch_l1((const char *)(t < 8 ? work.src0 : work.src1) + (size_t)sx * (BITS == 8 ? 1 : 2));
+        }
         line_twiddle(v, a.twN, r, t);
         line_sum(v);
 #pragma unroll
