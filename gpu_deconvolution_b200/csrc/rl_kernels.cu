@@ -130,8 +130,9 @@ __device__ __forceinline__ void store_sample(void *base, size_t idx, float v, in
 // branches.  NOOUT: an update pass known at compile time not to be the last
 // one, so the output-sample code is left out.  SMEM (with BITS fixed): the
 // operand rows are in shared memory at the s_* addresses (the data rows in
-// the divide pass; the estimate and weight rows in the update pass).
-template <int MODE, int BITS = 0, bool NOOUT = false, bool SMEM = false>
+// the divide pass; the weight row in the update pass, and the estimate row
+// too when EST_S).
+template <int MODE, int BITS = 0, bool NOOUT = false, bool SMEM = false, bool EST_S = SMEM>
 struct RowWork {
     const RlDims &d;
     float2 *est;             // row y of the pair's estimate (global)
@@ -220,7 +221,10 @@ struct RowWork {
             float2 c;
             if constexpr (SMEM) {
                 w = lds_f32(s_w + 4u * sx);
-                c = lds_f32x2(s_est + 8u * x);
+                if constexpr (EST_S)
+                    c = lds_f32x2(s_est + 8u * x);
+                else
+                    c = est[x];
             } else if constexpr (BITS != 0) {
                 w = wrow[sx];
                 c = (est_s ? est_s : est)[x];
@@ -692,7 +696,9 @@ __device__ __forceinline__ float2 line_coefficient(const float2 *__restrict__ tw
 
 // Row pass for W = R * 512: R warps, two rows per block (half-warp h of warp
 // r is group r of row h).
-template <int R, int MODE, int BITS, bool NOOUT>
+// SMEM: the launch bulk-copies each row's weight row (update) or data rows
+// (divide) into shared memory after the buffers.
+template <int R, int MODE, int BITS, bool NOOUT, bool SMEM>
 __global__ void __launch_bounds__(R * 32, 16 / R) row_pass_r(const RowArgs a)
 {
     using WF = WarpFft<kLineM>;
@@ -707,7 +713,29 @@ __global__ void __launch_bounds__(R * 32, 16 / R) row_pass_r(const RowArgs a)
     const int y = blockIdx.x * 2 + h;
     const int p = blockIdx.y;
     float2 *row = a.b.C + ((size_t)p * a.d.H + y) * N + r * kLineM;
-    RowWork<MODE, BITS, NOOUT> work(a, p, y);
+    RowWork<MODE, BITS, NOOUT, SMEM, false> work(a, p, y);
+
+    // operand rows staged by bulk copies, issued now by one thread per row
+    constexpr bool staged = SMEM && MODE != ROW_INIT;
+    __shared__ __align__(8) uint64_t sbar[2];
+    const uint32_t rb = a.d.dataW * (MODE == ROW_UPDATE ? (uint32_t)sizeof(float) : (BITS == 8 ? 1u : 2u));
+    const uint32_t rs = (rb + 15) & ~15u;
+    char *const st = reinterpret_cast<char *>(smem) + sizeof(float2) * 2 * R * PF2 +
+                     (size_t)h * (MODE == ROW_UPDATE ? rs : 2 * rs);
+    if (staged && threadIdx.x == 16 * h) {
+        mbar_init(&sbar[h], 1);
+        mbar_fence_init();
+        if (MODE == ROW_UPDATE) {
+            mbar_arrive_expect_tx(&sbar[h], rb);
+            bulk_load(st, work.wrow, rb, &sbar[h]);
+        } else {
+            mbar_arrive_expect_tx(&sbar[h], work.has1 ? 2 * rb : rb);
+            bulk_load(st, work.src0, rb, &sbar[h]);
+            if (work.has1)
+                bulk_load(st + rs, work.src1, rb, &sbar[h]);
+        }
+    }
+
     // the sum over the row's R groups: v[m] = sum_j (group j's v[m]) w_R^(r j)
     const auto line_sum = [&](float2 *v) {
 #pragma unroll
@@ -758,13 +786,29 @@ __global__ void __launch_bounds__(R * 32, 16 / R) row_pass_r(const RowArgs a)
         if (MODE == ROW_UPDATE) {
             prefetch_l1(work.est + r * kLineM + 16 * t);
             prefetch_l1(work.est + r * kLineM + 16 * (t + 16));
-            prefetch_l1(work.wrow + clamp_src(r * kLineM + 32 * t, a.d.dataW, a.d.bxW));
-        } else if (MODE == ROW_DIVIDE) {
+            if (!staged)
+                prefetch_l1(work.wrow + clamp_src(r * kLineM + 32 * t, a.d.dataW, a.d.bxW));
+        } else if (MODE == ROW_DIVIDE && !staged) {
             const int sx = clamp_src(r * kLineM + 64 * (t & 7), a.d.dataW, a.d.bxD);
             prefetch_l1((const char *)(t < 8 ? work.src0 : work.src1) + (size_t)sx * (BITS == 8 ? 1 : 2));
         }
         line_twiddle(v, a.twN, r, t);
         line_sum(v);
+        if (staged) {
+            if (!mbar_wait(&sbar[h], 0)) {
+                // the copy did not land in time: flag it (the host reports the
+                // batch as failed) and wait once more so no copy is left in flight
+                if (threadIdx.x == 16 * h)
+                    atomicExch(a.b.status, 1);
+                mbar_wait(&sbar[h], 0);
+            }
+            if (MODE == ROW_UPDATE) {
+                work.s_w = smem_u32addr(st);
+            } else {
+                work.s_src0 = smem_u32addr(st);
+                work.s_src1 = work.has1 ? smem_u32addr(st + rs) : work.s_src0;
+            }
+        }
 #pragma unroll
         for (int m = 0; m < E; m++) {
             v[m].y = -v[m].y;
@@ -1130,21 +1174,31 @@ static void pick_row_w(bool noout, bool sm, void (*&kern)(const RowArgs), unsign
 
 // Line-engine row-pass variant for a launch (per sample width; update
 // passes per last / not last).
-template <int R, int MODE>
-static void pick_row_r(const RowArgs &a, void (*&kern)(const RowArgs), unsigned *&m)
+template <int R, int MODE, int BITS>
+static void pick_row_r_bits(bool noout, bool sm, void (*&kern)(const RowArgs), unsigned *&m)
 {
-    static unsigned mask[5] = {0, 0, 0, 0, 0};
-    const bool noout = MODE == ROW_UPDATE && !a.last;
+    static unsigned mask[4] = {0, 0, 0, 0};
     constexpr bool U = MODE == ROW_UPDATE;
+    if (noout)
+        kern = sm ? row_pass_r<R, MODE, BITS, U, true> : row_pass_r<R, MODE, BITS, U, false>;
+    else
+        kern = sm ? row_pass_r<R, MODE, BITS, false, true> : row_pass_r<R, MODE, BITS, false, false>;
+    m = &mask[(noout ? 1 : 0) + (sm ? 2 : 0)];
+}
+
+// (sm: the operand rows may be bulk-copied into shared memory)
+template <int R, int MODE>
+static void pick_row_r(const RowArgs &a, bool sm, void (*&kern)(const RowArgs), unsigned *&m)
+{
+    static unsigned mask0 = 0;
+    const bool noout = MODE == ROW_UPDATE && !a.last;
     if constexpr (MODE == ROW_INIT) {
-        kern = row_pass_r<R, MODE, 0, false>;
-        m = &mask[0];
+        kern = row_pass_r<R, MODE, 0, false, false>;
+        m = &mask0;
     } else if (a.d.bits == 16) {
-        kern = noout ? row_pass_r<R, MODE, 16, U> : row_pass_r<R, MODE, 16, false>;
-        m = &mask[noout ? 3 : 1];
+        pick_row_r_bits<R, MODE, 16>(noout, sm, kern, m);
     } else {
-        kern = noout ? row_pass_r<R, MODE, 8, U> : row_pass_r<R, MODE, 8, false>;
-        m = &mask[noout ? 4 : 2];
+        pick_row_r_bits<R, MODE, 8>(noout, sm, kern, m);
     }
 }
 
@@ -1190,13 +1244,24 @@ static void launch_row(const RowArgs &a0, cudaStream_t s)
     } else {
         constexpr int R = W / kLineM;
         static_assert(W % kLineM == 0 && R >= 3 && R <= 8, "rows above 1024 are 3..8 sub-lines of 512");
-        const size_t smem = sizeof(float2) * 2 * R * WarpFft<kLineM>::padded_f2;
+        RowArgs a = a0;
+        const size_t es = a.d.bits == 16 ? 2 : 1;
+        a.bulk_data = aligned16(a.b.data, a.d.dataW * es) && (a.b.view_stride * es) % 16 == 0 &&
+                      (a.b.plane_stride * es) % 16 == 0;
+        a.bulk_weights = aligned16(a.b.weights, a.d.dataW * sizeof(float)) &&
+                         ((size_t)a.d.dataH * a.d.dataW * sizeof(float)) % 16 == 0;
+        const bool sm = MODE == ROW_UPDATE ? a.bulk_weights != 0 : (MODE == ROW_DIVIDE && a.bulk_data != 0);
+        size_t smem = sizeof(float2) * 2 * R * WarpFft<kLineM>::padded_f2;
+        if (sm) {
+            const size_t rs = ((size_t)a.d.dataW * (MODE == ROW_UPDATE ? sizeof(float) : es) + 15) & ~(size_t)15;
+            smem += 2 * (MODE == ROW_UPDATE ? rs : 2 * rs);
+        }
         void (*kern)(const RowArgs);
         unsigned *m;
-        pick_row_r<R, MODE>(a0, kern, m);
-        configure_smem(kern, smem, *m);
-        dim3 grid(a0.d.H / 2, a0.b.npairs);
-        kern<<<grid, R * 32, smem, s>>>(a0);
+        pick_row_r<R, MODE>(a, sm, kern, m);
+        configure_smem(kern, 200 * 1024, *m);
+        dim3 grid(a.d.H / 2, a.b.npairs);
+        kern<<<grid, R * 32, smem, s>>>(a);
     }
     g_launches++;
 }
