@@ -65,9 +65,9 @@ def parse():
     p.add_argument("--workload", default="transform_rl", choices=["transform_rl", "warmstart", "batched", "planes"],
                    help="warmstart: learned warm start vs plain RL-50 (time to the RL-50 result); planes: plain "
                         "RL throughput per padded plane size (--planes)")
-    p.add_argument("--planes", default="1536,2560",
+    p.add_argument("--planes", default="1400,2048",
                    help="planes workload: comma-separated data plane sizes, each padded by a 31 x 31 kernel "
-                        "(63 x 63 above 2000): 1400 -> 1536, 2300 -> 2560")
+                        "(63 x 63 from 2000 up): 900 -> 1024, 1400 -> 1536, 2048 -> 2560 FFT planes")
     p.add_argument("--pairs-per-batch", type=int, default=0,
                    help="planes workload: plane pairs per batch (0: the library's default)")
     p.add_argument("--train-planes", type=int, default=4000)
@@ -608,7 +608,7 @@ def run_planes(args):
     from gpu_deconvolution_b200 import api, synth
     V, IT = 4, 2 if args.small else 10
     for size in [int(x) for x in args.planes.split(",") if x]:
-        k = 63 if size > 2000 else 31
+        k = 63 if size >= 2000 else 31
         psfs = [synth.gaussian_psf(k, k, 1.2, 5.0, 45.0 * v) for v in range(V)]
         weights = [np.ones((size, size), np.float32) for _ in range(V)]
         plan = api.DevicePlan(size, size, weights, [q.copy() for q in psfs], 0,
