@@ -50,6 +50,8 @@ ZSCALE = 3.0
 BORDER = 16
 BYTES_PER_PADDED_VOXEL_VIEW_ITER = 14  # read e (4) + write e (4) + data (2) + weight (4)
 METRIC = "RL voxel-iter/s"
+WORKLOAD_NAME = ("transform + plain RL: 4 views u16 512x512x128 (z spacing 3) -> 512x512x384 frame, 20 RL "
+                 "iterations, 31x31 PSFs, FFT plane 1024x1024")
 UNIT = "voxel-iter/s"
 
 
@@ -335,9 +337,7 @@ def run_b200(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "transform + plain RL: 4 views u16 512x512x128 (z spacing 3) -> 512x512x384 "
-                                   "frame, 20 RL iterations, 31x31 PSFs, FFT plane 1024x1024" +
-                                   (" [small]" if args.small else ""),
+            "config": {"workload": WORKLOAD_NAME + (" [small]" if args.small else ""),
                        "views": V, "frame": list(frame), "iterations": ITERATIONS, "fft_plane": [H, W],
                        "pairs_per_batch": plan.pairs_per_batch,
                        "l2": "inputs larger than L2 (268 MB of source views per step)",
@@ -411,57 +411,58 @@ def run_e2e(args, vols, mats, psfs, weights, src, frame, world=1):
 
 # ------------------------------------------------------------ reference
 def run_reference(args):
-    import ctypes as C
+    """The reference's own implementation of the path, timed on the same
+    workload: the upstream deconvolution sources built for sm_100a with cuFFT
+    (oracle/_ref/libfmvd_ref.so, through fmvd_initialize / deconvolve_planes /
+    destroy with C callbacks, nstreams 3) and the texture-unit restatement of
+    its resampler and mask kernel (oracle/_ref/libfmvd_reftex.so), host
+    buffers in and out.  Nothing of this project's library is loaded."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    ref = os.path.join(ROOT, "oracle", "_ref", "libfmvd_ref.so")
-    tex_path = os.path.join(ROOT, "oracle", "_ref", "libfmvd_reftex.so")
-    if not (os.path.exists(ref) and os.path.exists(tex_path)):
+    from oracle import ref_lib as R
+    if not R.available():
         print(json.dumps({"impl": "reference", "unavailable": "reference build (oracle/_ref) not present"}))
         return
     import torch
     torch.cuda.set_device(0)
-    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
-    import make_golden
-    lib, tex = make_golden.load_ref()
+    lib, tex = R.load_ref()
     vols, mats, psfs, src, frame = workload(1234, args.small)
-    weights = masks_for(mats, src, frame)
     d, h, w = src
     td, th, tw = frame
+    weights = [R.ref_mask(tex, m, td // 2, w, h, d, ZSCALE, tw, th, BORDER) for m in mats]
 
     def step():
-        frames = np.zeros((V, td, th, tw), np.uint16)
-        for v in range(V):
-            m = np.ascontiguousarray(mats[v])
-            r = tex.reftex_transform(16, np.ascontiguousarray(vols[v]).ctypes.data, w, h, d, tw, th, td,
-                                     m.ctypes.data, frames[v].ctypes.data, None, None)
-            assert r == 0
-        res = make_golden.ref_deconvolve(lib, frames, weights, [p.copy() for p in psfs], 0, ITERATIONS, 3, False)
+        frames = np.stack([R.ref_transform(tex, vols[v], mats[v], tw, th, td) for v in range(V)])
+        res = R.ref_deconvolve(lib, frames, weights, [p.copy() for p in psfs], 0, ITERATIONS, 3, False)
+        assert res["out"].shape[0] == td
         return res["out"]
 
-    for _ in range(min(args.warmup, 1)):
+    for _ in range(args.warmup):
         step()
-    t0 = time.perf_counter()
-    n = max(1, min(args.steps, 2))
-    for _ in range(n):
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         step()
-    dt = (time.perf_counter() - t0) / n
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    dt = sum(times) / len(times)
     value = td * th * tw * ITERATIONS / dt
     h2d = V * d * h * w * 2 + V * td * th * tw * 2
     d2h = V * td * th * tw * 2 + td * th * tw * 2
     print(json.dumps({
-        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": 1, "steps": n,
-        "warmup": min(args.warmup, 1), "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "transform + plain RL: 4 views u16 512x512x128 (z spacing 3) -> 512x512x384 frame, "
-                               "20 RL iterations, 31x31 PSFs, FFT plane 1024x1024" + (" [small]" if args.small else ""),
+        "config": {"workload": WORKLOAD_NAME + (" [small]" if args.small else ""),
                    "views": V, "frame": list(frame), "iterations": ITERATIONS},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 0, "kind": "reference",
-                         "sample": "the reference's own implementation, which is CUDA: upstream deconvolution "
-                                   "sources built for sm_100a with cuFFT (nstreams 3) and the texture-unit "
-                                   "restatement of its resampler, host buffers in and out, on 1 B200"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": "the whole workload per step through the reference's own implementation, which "
+                                   "is CUDA: upstream deconvolution sources built for sm_100a with cuFFT (nstreams 3, "
+                                   "C callbacks) and the texture-unit restatement of its resampler and mask, host "
+                                   "buffers in and out, one host thread driving 1 B200"},
     }), flush=True)
 
 

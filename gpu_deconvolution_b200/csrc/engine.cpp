@@ -6,8 +6,9 @@
 // then the caller's kernels normalised in place (fmvd_deconvolve.impl.cpp:63-64),
 // kernel spectra, and weights normalised over views
 // (fmvd_deconvolve.impl.cpp:86-124).  Spectra are computed on the device by a
-// direct separable DFT in double precision; the small same-size convolutions
-// of the compound kernels run on the device in double precision too.
+// direct separable DFT in FP32 with compensated sums; the small same-size
+// convolutions of the compound kernels run on the device in FP32 too.  (FP64
+// on the GPU is used only by the convergence statistics.)
 #include "fmvd_internal.h"
 
 #include <math.h>
@@ -38,22 +39,17 @@ void invert_kernel(const float *k, float *out, int kw, int kh)
             out[y * kw + x] = k[(kh - y - 1) * kw + (kw - x - 1)];
 }
 
-// Clamp-padded circular convolution of a kernel-sized image on the device
-// (the reference's convolve_single_plane, fmvd_deconvolve.cpp:90-137).
-bool conv_same(float *img, const float *k, int kw, int kh, double *d_a, double *d_b, double *d_c)
+// Clamp-padded circular convolution of a kernel-sized image on the device in
+// FP32 (the reference's convolve_single_plane, fmvd_deconvolve.cpp:90-137,
+// an FP32 cuFFT convolution).
+bool conv_same(float *img, const float *k, int kw, int kh, float *d_a, float *d_b, float *d_c)
 {
-    const int n = kw * kh;
-    std::vector<double> a(img, img + n), b(k, k + n), c(n);
-    if (!FMVD_CHECK(cudaMemcpy(d_a, a.data(), n * sizeof(double), cudaMemcpyHostToDevice)) ||
-        !FMVD_CHECK(cudaMemcpy(d_b, b.data(), n * sizeof(double), cudaMemcpyHostToDevice)))
+    const size_t bytes = sizeof(float) * kw * kh;
+    if (!FMVD_CHECK(cudaMemcpy(d_a, img, bytes, cudaMemcpyHostToDevice)) ||
+        !FMVD_CHECK(cudaMemcpy(d_b, k, bytes, cudaMemcpyHostToDevice)))
         return false;
     rl_conv_same(d_a, kh, kw, d_b, kh, kw, d_c, 0);
-    if (!FMVD_CHECK(cudaGetLastError()) ||
-        !FMVD_CHECK(cudaMemcpy(c.data(), d_c, n * sizeof(double), cudaMemcpyDeviceToHost)))
-        return false;
-    for (int i = 0; i < n; i++)
-        img[i] = (float)c[i];
-    return true;
+    return FMVD_CHECK(cudaGetLastError()) && FMVD_CHECK(cudaMemcpy(img, d_c, bytes, cudaMemcpyDeviceToHost));
 }
 
 // fmvd_deconvolve.cpp:139-204
@@ -62,12 +58,15 @@ bool compute_kernel2(float *const *k, int kw, int kh, int V, int type, std::vect
     const int n = kw * kh;
     k2.assign(V, std::vector<float>(n));
     std::vector<float> t1(n), t2(n);
-    double *d_a = nullptr, *d_b = nullptr, *d_c = nullptr;
+    float *d_a = nullptr, *d_b = nullptr, *d_c = nullptr;
     bool need_conv = (type == efficient_bayesian || type == optimization_1) && V > 1;
     if (need_conv) {
-        if (!FMVD_CHECK(cudaMalloc(&d_a, n * sizeof(double))) || !FMVD_CHECK(cudaMalloc(&d_b, n * sizeof(double))) ||
-            !FMVD_CHECK(cudaMalloc(&d_c, n * sizeof(double))))
+        if (!FMVD_CHECK(cudaMalloc(&d_a, n * sizeof(float))) || !FMVD_CHECK(cudaMalloc(&d_b, n * sizeof(float))) ||
+            !FMVD_CHECK(cudaMalloc(&d_c, n * sizeof(float)))) {
+            cudaFree(d_a);
+            cudaFree(d_b);
             return false;
+        }
     }
     bool ok = true;
     for (int v = 0; v < V && ok; v++) {
@@ -268,28 +267,23 @@ Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weig
              FMVD_CHECK(cudaMemcpy(e->wtwH, wH.data(), sizeof(float2) * wH.size(), cudaMemcpyHostToDevice)) &&
              FMVD_CHECK(cudaMemcpy(e->wtwW, wW.data(), sizeof(float2) * wW.size(), cudaMemcpyHostToDevice));
 
-        // kernel spectra
-        double2 *d_twH = nullptr, *d_twW = nullptr, *work = nullptr;
+        // kernel spectra (FP32 on the device; the twiddle tables are the
+        // float tables above, computed in double on the host and rounded)
+        float2 *work = nullptr;
         float *d_k = nullptr;
-        ok = ok && FMVD_CHECK(cudaMalloc(&d_twH, sizeof(double2) * H)) &&
-             FMVD_CHECK(cudaMalloc(&d_twW, sizeof(double2) * W)) &&
-             FMVD_CHECK(cudaMalloc(&work, sizeof(double2) * ((size_t)H * W + (size_t)kH * W))) &&
-             FMVD_CHECK(cudaMalloc(&d_k, sizeof(float) * kH * kW)) &&
-             FMVD_CHECK(cudaMemcpy(d_twH, tH.data(), sizeof(double2) * H, cudaMemcpyHostToDevice)) &&
-             FMVD_CHECK(cudaMemcpy(d_twW, tW.data(), sizeof(double2) * W, cudaMemcpyHostToDevice));
+        ok = ok && FMVD_CHECK(cudaMalloc(&work, sizeof(float2) * ((size_t)H * W + (size_t)kH * W))) &&
+             FMVD_CHECK(cudaMalloc(&d_k, sizeof(float) * kH * kW));
         for (int v = 0; v < nViews && ok; v++) {
             for (int which = 0; which < 2 && ok; which++) {
                 const float *src = which == 0 ? h_Kernel[v] : k2[v].data();
                 ok = FMVD_CHECK(cudaMemcpy(d_k, src, sizeof(float) * kH * kW, cudaMemcpyHostToDevice));
                 if (ok) {
-                    rl_kernel_spectrum(d_k, kH, kW, H, W, d_twH, d_twW, work,
+                    rl_kernel_spectrum(d_k, kH, kW, H, W, e->twH, e->twW, work,
                                        e->spec + e->spec_elems * (2 * v + which), e->dims.col_warps, 0);
                     ok = FMVD_CHECK(cudaGetLastError()) && FMVD_CHECK(cudaDeviceSynchronize());
                 }
             }
         }
-        cudaFree(d_twH);
-        cudaFree(d_twW);
         cudaFree(work);
         cudaFree(d_k);
     }

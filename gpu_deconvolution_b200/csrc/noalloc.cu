@@ -2,16 +2,19 @@
 // a plan with its work memory taken from a fixed array of this library, so the
 // call itself allocates nothing.
 //
-// Why: fmvd_b200_deconvolve_device runs in the plan's own work planes (two
-// complex planes per batched plane pair: 16 MiB per pair at 1024 x 1024, and
-// the automatic batch holds several pairs), sized when the plan is created.
-// A caller that keeps many plans alive at once (one per view configuration or
-// plane size) and has no device memory to spare for each plan's full batch of
-// work planes -- the rest of the GPU already holds its frame buffers, or
-// another allocator has reserved it -- creates its plans with
-// pairs_per_batch = 1 and deconvolves through this entry point, whose work
-// planes live in one array shared by every plan and reserved when the
-// library's module is loaded on a device.  Nothing here calls cudaMalloc,
+// Why: some callers cannot call cudaMalloc at the point where they
+// deconvolve.  A host framework that owns the device's free memory through
+// its own pool, a real-time acquisition loop that must not take the
+// allocator's device-wide synchronisation, or a plugin running inside another
+// application's CUDA context may only hand this library buffers it already
+// holds.  fmvd_b200_deconvolve_device itself allocates nothing either, but it
+// runs in work planes the plan allocated at creation, sized for the plan's
+// batch and lanes; this entry point runs in one array of this library that
+// the CUDA runtime reserves when it loads the library's module on a device,
+// so the call needs no memory beyond the plan's spectra and weights and the
+// caller's inputs and outputs.  The plan still holds its own work planes
+// (created with pairs_per_batch = 1 they are the smallest the plan allows);
+// this entry point does not use them.  Nothing here calls cudaMalloc,
 // cudaFree or any routine that allocates.
 //
 // Limit: the array is kScratchBytes (64 MiB).  Its first 256 bytes hold the
@@ -20,48 +23,39 @@
 // fit one pair (more than about 4.19 M complex points, e.g. 2048 x 2048) is
 // rejected with an error.
 //
+// Device: the call must be made with the plan's device current (the array is
+// per device); another current device is rejected.  The array's device
+// address is looked up on every call (cudaGetSymbolAddress allocates
+// nothing).  The first call on a device may make the runtime load the
+// library's module there, so make that first call before any stream capture.
+//
 // Sharing: every call on a device uses the same array, and the array keeps
 // the last call's contents.  The status word is cleared at the start of each
 // call; the work planes are written before they are read.  Calls that
 // overlap in time on one device (from two host threads, or queued on two
 // streams) race on the array and corrupt each other's results: serialise them.
+// The call returns only when its work on the stream has finished, on success
+// and on failure, so consecutive calls from one thread never overlap.
 #include "fmvd_b200.h"
 #include "fmvd_internal.h"
 
-#include <mutex>
 #include <stdio.h>
 
 namespace {
 
 constexpr size_t kScratchBytes = size_t(64) << 20;
 constexpr size_t kStatusBytes = 256;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-std::mutex g_setup_lock;
-void *g_scratch_addr[kMaxDevices];
-
-// Device address of g_scratch on the current device, looked up once per
-// device (the first call on a device does this set-up; make that first call
-// before any stream capture).  Null after reporting an error.
+// Device address of g_scratch on the current device (an error is reported
+// and null returned if the lookup fails).
 void *scratch_address()
 {
-    int dev = -1;
-    if (!FMVD_CHECK(cudaGetDevice(&dev)))
+    void *p = nullptr;
+    if (!FMVD_CHECK(cudaGetSymbolAddress(&p, g_scratch)))
         return nullptr;
-    if (dev < 0 || dev >= kMaxDevices) {
-        fmvd::report_error("fmvd: fmvd_b200_deconvolve_device_noalloc supports device ordinals below 64");
-        return nullptr;
-    }
-    std::lock_guard<std::mutex> guard(g_setup_lock);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        if (!FMVD_CHECK(cudaGetSymbolAddress(&p, g_scratch)))
-            return nullptr;
-        g_scratch_addr[dev] = p;
-    }
-    return g_scratch_addr[dev];
+    return p;
 }
 
 } // namespace
@@ -87,6 +81,17 @@ extern "C" int fmvd_b200_deconvolve_device_noalloc(fmvd_b200_plan *plan, const v
         fmvd::report_error(msg);
         return 1;
     }
+    int dev = -1;
+    if (!FMVD_CHECK(cudaGetDevice(&dev)))
+        return 1;
+    if (dev != e->device) {
+        char msg[200];
+        snprintf(msg, sizeof msg,
+                 "fmvd: fmvd_b200_deconvolve_device_noalloc: the plan lives on device %d but device %d is current",
+                 e->device, dev);
+        fmvd::report_error(msg);
+        return 1;
+    }
     char *base = static_cast<char *>(scratch_address());
     if (!base)
         return 1;
@@ -103,8 +108,12 @@ extern "C" int fmvd_b200_deconvolve_device_noalloc(fmvd_b200_plan *plan, const v
 
     if (!FMVD_CHECK(cudaMemsetAsync(run.status, 0, sizeof(int), s)))
         return 1;
-    if (!fmvd::engine_run(&run, d_views, view_stride, d_out, nplanes, iterations, d_estimate, s))
+    if (!fmvd::engine_run(&run, d_views, view_stride, d_out, nplanes, iterations, d_estimate, s)) {
+        // kernels queued before the failure still use the array: let them
+        // finish so that the array is idle when this call returns
+        cudaStreamSynchronize(s);
         return 1;
+    }
     // The status word is reused by the next call, so it is read before
     // returning: the call waits for its work on the stream to finish.
     int status = 0;

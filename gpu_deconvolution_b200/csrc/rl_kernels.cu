@@ -965,7 +965,7 @@ __host__ __device__ __forceinline__ int stored_frequency(int j, int n)
 // Launch layout of the line engine's column-pass spectrum: block bx
 // (stored columns 2 bx, 2 bx + 1), register m, thread tid = 32 r + 16 cc + t
 // holds frequency ky = R (t + 16 m) + r of stored column 2 bx + cc.
-__global__ void permute_spectrum_r(const double2 *__restrict__ nat, float2 *__restrict__ out, int H, int W, double scale)
+__global__ void permute_spectrum_r(const float2 *__restrict__ nat, float2 *__restrict__ out, int H, int W, float scale)
 {
     const int R = H / kLineM, NT = 32 * R;
     const size_t total = (size_t)H * W;
@@ -976,14 +976,14 @@ __global__ void permute_spectrum_r(const double2 *__restrict__ nat, float2 *__re
         const int r = tid >> 5, cc = (tid >> 4) & 1, t = tid & 15;
         const int ky = R * (t + 16 * m) + r;
         const int kx = stored_frequency(2 * bx + cc, W);
-        const double2 k = nat[(size_t)ky * W + kx];
-        out[i] = make_float2((float)(k.x * scale), (float)(k.y * scale));
+        const float2 k = nat[(size_t)ky * W + kx];
+        out[i] = make_float2(k.x * scale, k.y * scale);
     }
 }
 
 // Launch layout of the column-pass spectrum for the warp engine.
-__global__ void permute_spectrum_w(const double2 *__restrict__ nat, float2 *__restrict__ out, int H, int W, int T,
-                                   int CW, double scale)
+__global__ void permute_spectrum_w(const float2 *__restrict__ nat, float2 *__restrict__ out, int H, int W, int T,
+                                   int CW, float scale)
 {
     const int E = H / T, G = 32 / T, FC = CW * G, NT = CW * 32;
     const size_t total = (size_t)H * W;
@@ -995,51 +995,68 @@ __global__ void permute_spectrum_w(const double2 *__restrict__ nat, float2 *__re
         const int g = lane / T, t = lane % T;
         const int n = t + T * m;
         const int col = stored_frequency(bx * FC + warp * G + g, W);
-        const double2 k = nat[(size_t)n * W + col];
-        out[i] = make_float2((float)(k.x * scale), (float)(k.y * scale));
+        const float2 k = nat[(size_t)n * W + col];
+        out[i] = make_float2(k.x * scale, k.y * scale);
     }
 }
 
+// Plan-time kernels in FP32 (the reference builds its kernel spectra with an
+// FP32 cuFFT, fmvd_deconvolve.impl.cpp:66-76).  Sums use compensated
+// (Kahan) accumulation with explicitly rounded operations, so that the
+// spectra carry about FP32 rounding of the exact value whatever the kernel
+// size.
+struct KahanSum {
+    float s = 0.f, c = 0.f;
+    __device__ __forceinline__ void add(float v)
+    {
+        const float y = __fsub_rn(v, c);
+        const float t = __fadd_rn(s, y);
+        c = __fsub_rn(__fsub_rn(t, s), y);
+        s = t;
+    }
+};
 
 // Separable direct DFT of a small kernel placed at (y - kH/2, x - kW/2) mod (H, W).
 // Step 1: A[y][v] = sum_x k[y][x] exp(-2 pi i v (x - cx) / W)
-__global__ void kspec_rows(const float *__restrict__ k, int kH, int kW, int W, const double2 *__restrict__ twW,
-                           double2 *__restrict__ A)
+__global__ void kspec_rows(const float *__restrict__ k, int kH, int kW, int W, const float2 *__restrict__ twW,
+                           float2 *__restrict__ A)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (v >= W)
         return;
-    double re = 0, im = 0;
+    KahanSum re, im;
     const int cx = kW / 2;
     for (int x = 0; x < kW; x++) {
         const long long ph = ((long long)v * (x - cx)) % W;
-        const double2 t = twW[ph < 0 ? ph + W : ph];
-        const double kv = k[y * kW + x];
-        re += kv * t.x;
-        im += kv * t.y;
+        const float2 t = twW[ph < 0 ? ph + W : ph];
+        const float kv = k[y * kW + x];
+        re.add(__fmul_rn(kv, t.x));
+        im.add(__fmul_rn(kv, t.y));
     }
-    A[(size_t)y * W + v] = make_double2(re, im);
+    A[(size_t)y * W + v] = make_float2(re.s, im.s);
 }
 
 // Step 2: K[u][v] = sum_y A[y][v] exp(-2 pi i u (y - cy) / H)
-__global__ void kspec_cols(const double2 *__restrict__ A, int kH, int H, int W, const double2 *__restrict__ twH,
-                           double2 *__restrict__ K)
+__global__ void kspec_cols(const float2 *__restrict__ A, int kH, int H, int W, const float2 *__restrict__ twH,
+                           float2 *__restrict__ K)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     const int u = blockIdx.y;
     if (v >= W)
         return;
-    double re = 0, im = 0;
+    KahanSum re, im;
     const int cy = kH / 2;
     for (int y = 0; y < kH; y++) {
         const long long ph = ((long long)u * (y - cy)) % H;
-        const double2 t = twH[ph < 0 ? ph + H : ph];
-        const double2 a = A[(size_t)y * W + v];
-        re += a.x * t.x - a.y * t.y;
-        im += a.x * t.y + a.y * t.x;
+        const float2 t = twH[ph < 0 ? ph + H : ph];
+        const float2 a = A[(size_t)y * W + v];
+        re.add(__fmul_rn(a.x, t.x));
+        re.add(-__fmul_rn(a.y, t.y));
+        im.add(__fmul_rn(a.x, t.y));
+        im.add(__fmul_rn(a.y, t.x));
     }
-    K[(size_t)u * W + v] = make_double2(re, im);
+    K[(size_t)u * W + v] = make_float2(re.s, im.s);
 }
 
 __global__ void normalize_weights_kernel(const float *__restrict__ in, float *__restrict__ out, int V, size_t n)
@@ -1060,14 +1077,14 @@ __device__ __forceinline__ int clamp_src_d(int i, int n, int border)
     return i < n ? i : (i < n + border ? n - 1 : 0);
 }
 
-__global__ void conv_same_kernel(const double *__restrict__ img, int dH, int dW, const double *__restrict__ k, int kH,
-                                 int kW, int fH, int fW, double *__restrict__ out)
+__global__ void conv_same_kernel(const float *__restrict__ img, int dH, int dW, const float *__restrict__ k, int kH,
+                                 int kW, int fH, int fW, float *__restrict__ out)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= dW || y >= dH)
         return;
-    double acc = 0;
+    KahanSum acc;
     for (int ky = 0; ky < kH; ky++) {
         int py = (y - (ky - kH / 2)) % fH;
         if (py < 0)
@@ -1078,10 +1095,10 @@ __global__ void conv_same_kernel(const double *__restrict__ img, int dH, int dW,
             if (px < 0)
                 px += fW;
             const int sx = clamp_src_d(px, dW, kW / 2);
-            acc += img[(size_t)sy * dW + sx] * k[ky * kW + kx];
+            acc.add(__fmul_rn(img[(size_t)sy * dW + sx], k[ky * kW + kx]));
         }
     }
-    out[(size_t)y * dW + x] = acc;
+    out[(size_t)y * dW + x] = acc.s;
 }
 
 // ------------------------------------------------------------ dispatch
@@ -1358,16 +1375,18 @@ int rl_warp_twiddle_entries(int n)
     return used > n ? used : n;
 }
 
-void rl_kernel_spectrum(const float *d_kernel, int kH, int kW, int H, int W, const double2 *twH, const double2 *twW,
-                        double2 *work, float2 *d_out, int cw, cudaStream_t s)
+void rl_kernel_spectrum(const float *d_kernel, int kH, int kW, int H, int W, const float2 *twH, const float2 *twW,
+                        float2 *work, float2 *d_out, int cw, cudaStream_t s)
 {
-    double2 *A = work;
-    double2 *K = work + (size_t)kH * W;
+    float2 *A = work;
+    float2 *K = work + (size_t)kH * W;
     kspec_rows<<<dim3((W + 127) / 128, kH), 128, 0, s>>>(d_kernel, kH, kW, W, twW, A);
     kspec_cols<<<dim3((W + 127) / 128, H), 128, 0, s>>>(A, kH, H, W, twH, K);
     const size_t total = rl_spectrum_elems(H, W);
     const int blocks = (int)((total + 255) / 256 > 4096 ? 4096 : (total + 255) / 256);
-    const double scale = 1.0 / ((double)H * (double)W);
+    // 1 / (H W), rounded once to float (the reference's modulateAndNormalize
+    // factor, fmvd_deconvolve_cuda.cu:369)
+    const float scale = (float)(1.0 / ((double)H * (double)W));
     if (H <= 1024) {
         permute_spectrum_w<<<blocks, 256, 0, s>>>(K, d_out, H, W, warp_fft_lanes(H), cw ? cw : col_warps(H, W),
                                                   scale);
@@ -1396,8 +1415,7 @@ void rl_normalize_weights(const float *d_in, float *d_out, int V, size_t n, cuda
     normalize_weights_kernel<<<blocks, 256, 0, s>>>(d_in, d_out, V, n);
 }
 
-void rl_conv_same(const double *d_img, int dH, int dW, const double *d_k, int kH, int kW, double *d_out,
-                  cudaStream_t s)
+void rl_conv_same(const float *d_img, int dH, int dW, const float *d_k, int kH, int kW, float *d_out, cudaStream_t s)
 {
     const int fH = snap_transform_size(dH + kH - 1);
     const int fW = snap_transform_size(dW + kW - 1);

@@ -77,19 +77,19 @@ void rl_write_estimate(const RlDims &d, const RlBatch &b, cudaStream_t s);
 // Float estimates of nplanes planes (H x W each) from the pair layout.
 void rl_split_estimate(const RlDims &d, const float2 *est, int nplanes, float *out, cudaStream_t s);
 
-// Plan-time helpers (device work, launched on stream s).
+// Plan-time helpers (device work in FP32, launched on stream s).
 // Kernel spectrum of a kH x kW kernel centred at (kH/2, kW/2) -> (0, 0) on the
 // H x W plane, scaled by 1 / (H W), in the column-pass launch layout.
-// work must hold 2 * H * W + kH * W complex doubles.
-// col_warps: the plan's column-pass warps (the launch layout depends on it).
-void rl_kernel_spectrum(const float *d_kernel, int kH, int kW, int H, int W, const double2 *twH, const double2 *twW,
-                        double2 *work, float2 *d_out, int col_warps, cudaStream_t s);
+// twH / twW: exp(-2 pi i n / N) tables; work must hold H * W + kH * W complex
+// floats.  col_warps: the plan's column-pass warps (the launch layout depends
+// on it).
+void rl_kernel_spectrum(const float *d_kernel, int kH, int kW, int H, int W, const float2 *twH, const float2 *twW,
+                        float2 *work, float2 *d_out, int col_warps, cudaStream_t s);
 // Weights normalised over views where the sum is positive.
 void rl_normalize_weights(const float *d_in, float *d_out, int V, size_t n, cudaStream_t s);
 // Clamp-to-border padded circular convolution of a dH x dW image with a
-// kH x kW kernel on the snapTransformSize domain, cropped to dH x dW (double).
-void rl_conv_same(const double *d_img, int dH, int dW, const double *d_k, int kH, int kW, double *d_out,
-                  cudaStream_t s);
+// kH x kW kernel on the snapTransformSize domain, cropped to dH x dW.
+void rl_conv_same(const float *d_img, int dH, int dW, const float *d_k, int kH, int kW, float *d_out, cudaStream_t s);
 
 int snap_transform_size(int n);
 

@@ -47,7 +47,9 @@ __device__ __forceinline__ void apply(const Mat &M, int x, int y, int z, float &
 // the nearest 1/256, halves up.
 __device__ __forceinline__ void tex_axis(float r, int &i, float &a)
 {
-    const float u = (float)((double)r + 0.5);
+    // the reference forms r + 0.5 in double and converts to float: the exact
+    // sum rounded once to float, which is what one float addition gives
+    const float u = __fadd_rn(r, 0.5f);
     const float fx = (u - 0.5f) * 256.0f;
     const float q = floorf(fx + 0.5f);
     const float fi = floorf(q * (1.0f / 256.0f));
@@ -66,9 +68,11 @@ __device__ __forceinline__ S quantise(float v)
 {
     // (SAMPLE)(v * 2^BITS + 0.5) as the reference compiles it: float product,
     // double sum, conversion through a 32-bit unsigned integer, so a fetch of
-    // exactly 1.0 wraps to 0 (measured on the B200)
-    const double q = (double)(v * (float)(1 << BITS)) + 0.5;
-    return (S)__double2uint_rz(q);
+    // exactly 1.0 wraps to 0 (measured on the B200).  The product is exact
+    // (a power of two) and below 2^23, where adding 0.5 in float is exact
+    // too, so float arithmetic gives the same integer.
+    const float q = __fadd_rn(v * (float)(1 << BITS), 0.5f);
+    return (S)__float2uint_rz(q);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -351,9 +355,50 @@ size_t source_pitch(int bits, int w)
     return ((size_t)w + a - 1) / a * a;
 }
 
+// Upload of d source planes (host pointers, any host memory) into the
+// pitched device volume: planes are packed into two pinned staging buffers in
+// turn, each staging buffer's copy to the device running while the host
+// packs the next.
+static bool upload_planes(const void *const *h_planes, int w, int h, int d, size_t es, size_t pitch, void *d_src,
+                          cudaStream_t s)
+{
+    const size_t row = (size_t)w * es, plane = row * h;
+    int per = (int)(((size_t)32 << 20) / (plane ? plane : 1));
+    per = per < 1 ? 1 : (per > d ? (d > 0 ? d : 1) : per);
+    void *stage[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    bool ok = true;
+    for (int k = 0; k < 2 && ok; k++)
+        ok = FMVD_CHECK(cudaMallocHost(&stage[k], plane * per)) &&
+             FMVD_CHECK(cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming));
+    bool used[2] = {false, false};
+    for (int z0 = 0, k = 0; ok && z0 < d; z0 += per, k ^= 1) {
+        const int n = d - z0 < per ? d - z0 : per;
+        if (used[k])
+            ok = FMVD_CHECK(cudaEventSynchronize(done[k]));  // the staging buffer's last copy has landed
+        for (int i = 0; ok && i < n; i++)
+            memcpy((char *)stage[k] + plane * i, h_planes[z0 + i], plane);
+        ok = ok && FMVD_CHECK(cudaMemcpy2DAsync((char *)d_src + pitch * h * z0 * es, pitch * es, stage[k], row, row,
+                                                (size_t)h * n, cudaMemcpyHostToDevice, s)) &&
+             FMVD_CHECK(cudaEventRecord(done[k], s));
+        used[k] = true;
+    }
+    if (ok)
+        ok = FMVD_CHECK(cudaStreamSynchronize(s));
+    else
+        cudaStreamSynchronize(s);
+    for (int k = 0; k < 2; k++) {
+        cudaFreeHost(stage[k]);
+        if (done[k])
+            cudaEventDestroy(done[k]);
+    }
+    return ok;
+}
+
 // transform_cuda_* (fmvd_transform.impl.cu:77-224): upload, optional mask of
 // plane td/2, resample in chunks of planes with download and file write of
-// one chunk overlapping the resampling of the next.
+// one chunk overlapping the resampling of the next.  Every buffer, event and
+// stream is released on every path.
 void transform_file(int bits, const void *const *h_planes, int w, int h, int d, int tw, int th, int td,
                     const float *h_inverse, const char *outfile, int masks, int border, float zspacing,
                     const char *maskfile)
@@ -362,17 +407,13 @@ void transform_file(int bits, const void *const *h_planes, int w, int h, int d, 
     const size_t pitch = source_pitch(bits, w);
     void *d_src = nullptr;
     int *d_status = nullptr;
-    if (!FMVD_CHECK(cudaMalloc(&d_src, pitch * h * d * es)) || !FMVD_CHECK(cudaMalloc(&d_status, sizeof(int))))
-        return;
-    FMVD_CHECK(cudaMemset(d_status, 0, sizeof(int)));
-    for (int z = 0; z < d; z++)
-        if (!FMVD_CHECK(cudaMemcpy2D((char *)d_src + pitch * h * z * es, pitch * es, h_planes[z], w * es, w * es, h,
-                                     cudaMemcpyHostToDevice)))
-            return;
-    cudaStream_t s;
-    FMVD_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    cudaStream_t s = nullptr;
+    bool ok = FMVD_CHECK(cudaMalloc(&d_src, pitch * h * d * es)) && FMVD_CHECK(cudaMalloc(&d_status, sizeof(int))) &&
+              FMVD_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) &&
+              FMVD_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), s)) &&
+              upload_planes(h_planes, w, h, d, es, pitch, d_src, s);
 
-    if (masks) {
+    if (ok && masks) {
         float *d_m = nullptr;
         std::vector<float> hm((size_t)tw * th);
         if (FMVD_CHECK(cudaMalloc(&d_m, sizeof(float) * tw * th)) &&
@@ -390,10 +431,10 @@ void transform_file(int bits, const void *const *h_planes, int w, int h, int d, 
         cudaFree(d_m);
     }
 
-    FILE *out = fopen(outfile, "wb");
-    if (!out) {
+    FILE *out = ok ? fopen(outfile, "wb") : nullptr;
+    if (ok && !out)
         report_error("fmvd: could not open the output file");
-    } else {
+    if (out) {
         const size_t plane_bytes = (size_t)tw * th * es;
         // The reference writes an unfilled slot ahead of the data when td < 2.
         if (td < 2) {
@@ -408,8 +449,7 @@ void transform_file(int bits, const void *const *h_planes, int w, int h, int d, 
             chunk = td > 0 ? td : 1;
         void *d_out[2] = {nullptr, nullptr};
         void *h_out[2] = {nullptr, nullptr};
-        cudaEvent_t ev[2];
-        bool ok = true;
+        cudaEvent_t ev[2] = {nullptr, nullptr};
         for (int k = 0; k < 2 && ok; k++)
             ok = FMVD_CHECK(cudaMalloc(&d_out[k], plane_bytes * chunk)) &&
                  FMVD_CHECK(cudaMallocHost(&h_out[k], plane_bytes * chunk)) &&
@@ -433,18 +473,23 @@ void transform_file(int bits, const void *const *h_planes, int w, int h, int d, 
             fwrite(h_out[pending_k], 1, plane_bytes * pending_n, out);
         }
         fclose(out);
+        cudaStreamSynchronize(s);
         for (int k = 0; k < 2; k++) {
             cudaFree(d_out[k]);
             cudaFreeHost(h_out[k]);
-            if (ok)
+            if (ev[k])
                 cudaEventDestroy(ev[k]);
         }
     }
-    int status = 0;
-    cudaMemcpy(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost);
-    if (status)
-        report_error("fmvd: a resampler brick load did not complete in time");
-    cudaStreamDestroy(s);
+    if (d_status) {
+        int status = 0;
+        if (s)
+            cudaStreamSynchronize(s);
+        if (cudaMemcpy(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && status)
+            report_error("fmvd: a resampler brick load did not complete in time");
+    }
+    if (s)
+        cudaStreamDestroy(s);
     cudaFree(d_src);
     cudaFree(d_status);
 }

@@ -24,15 +24,23 @@ import numpy as np
 
 
 def plane_range(n_planes: int, rank: int, world: int) -> tuple[int, int]:
-    """Contiguous share [z0, z1) of ``n_planes`` for ``rank`` of ``world``;
-    the first ``n_planes % world`` ranks take one plane more."""
+    """Contiguous share [z0, z1) of ``n_planes`` for ``rank`` of ``world``.
+
+    Planes are dealt in pairs (2p, 2p + 1), the pairs the library packs into
+    one complex transform, so every share starts at an even plane and each
+    plane keeps the partner it has in a whole-volume run: the assembled
+    result is then bit-identical to one GPU deconvolving the whole volume.
+    The first ``n_pairs % world`` ranks take one pair more; only the last
+    non-empty share can end on an unpaired plane (when ``n_planes`` is odd)."""
     if world < 1 or not 0 <= rank < world:
         raise ValueError(f"rank {rank} outside a world of {world}")
     if n_planes < 0:
         raise ValueError("negative plane count")
-    base, extra = divmod(n_planes, world)
-    z0 = rank * base + min(rank, extra)
-    return z0, z0 + base + (1 if rank < extra else 0)
+    pairs = (n_planes + 1) // 2
+    base, extra = divmod(pairs, world)
+    p0 = rank * base + min(rank, extra)
+    p1 = p0 + base + (1 if rank < extra else 0)
+    return min(2 * p0, n_planes), min(2 * p1, n_planes)
 
 
 def source_planes(inverse, w: int, h: int, d: int, tw: int, th: int, z0: int, z1: int) -> tuple[int, int]:
@@ -90,51 +98,94 @@ def gather_planes(local: np.ndarray, z0: int, n_planes: int, group=None):
 
 
 def run_shard(views, inverses, frame, kernels, weights, iterations, rank, world, psf_type=0, bits=16,
-              pairs_per_batch=0, stream=None):
-    """Resample and deconvolve this rank's target planes on the current CUDA
-    device.
+              pairs_per_batch=0, stream=None, resample=None, deconvolve=None):
+    """Resample and deconvolve this rank's target planes.
 
     views: list of V source volumes (d x h x w uint16/uint8, host arrays);
     inverses: V 3x4 target->source matrices; frame: (td, th, tw);
     kernels, weights, psf_type, iterations: as for ``fmvd_initialize_cuda_*``.
     Returns (z0, planes) with planes the rank's (z1 - z0) x th x tw result on
-    the host.  Only the source planes the range samples are copied to the
-    device; the rest of the source buffer is zero and never weighted.
-    """
-    import torch
+    the host.  Only the source planes the range samples are handed on; the
+    rest of each source volume is zero and never weighted.
 
-    from . import api
-
+    ``resample(v, slab, s0, inverse, z0, n)`` (slab: source planes
+    [s0, s0 + len(slab)) of view v) returns the resampled frame planes
+    [z0, z0 + n) of that view, and ``deconvolve(frames)`` (V x n x th x tw)
+    returns the n result planes; by default both run on the current CUDA
+    device through the native library (``DeviceShard``)."""
     td, th, tw = frame
     z0, z1 = plane_range(td, rank, world)
-    dtype = torch.int16 if bits == 16 else torch.uint8
-    npdt = np.int16 if bits == 16 else np.uint8
     n = z1 - z0
     out = np.zeros((n, th, tw), np.uint16 if bits == 16 else np.uint8)
     if n == 0:
         return z0, out
     V = len(views)
     d, h, w = views[0].shape
-    pitch = api.source_pitch(bits, w)
-    s = stream if stream is not None else torch.cuda.current_stream()
-    with torch.cuda.stream(s):
-        src = torch.zeros((d, h, pitch), dtype=dtype, device="cuda")
-        frame_dev = torch.empty((V, n, th, tw), dtype=dtype, device="cuda")
+    dev = None
+    if resample is None or deconvolve is None:
+        dev = DeviceShard(views[0].shape, frame, n, V, kernels, weights, psf_type, bits, pairs_per_batch, iterations,
+                          stream)
+        resample = resample or dev.resample
+        deconvolve = deconvolve or dev.deconvolve
+    try:
+        frames = []
         for v in range(V):
             s0, s1 = source_planes(inverses[v], w, h, d, tw, th, z0, z1)
-            src.zero_()
-            if s1 > s0:
-                slab = np.ascontiguousarray(views[v][s0:s1]).view(npdt)
-                src[s0:s1, :, :w].copy_(torch.from_numpy(slab).pin_memory(), non_blocking=True)
-            api.transform_device(src, pitch, w, h, d, inverses[v], tw, th, z0, n, out=frame_dev[v],
-                                 stream=s.cuda_stream, bits=bits)
-        res = torch.empty((n, th, tw), dtype=dtype, device="cuda")
-        plan = api.DevicePlan(th, tw, weights, [np.array(k, np.float32) for k in kernels], psf_type, bits=bits,
-                              pairs_per_batch=pairs_per_batch)
-        try:
-            plan.run(frame_dev, res, iterations, stream=s.cuda_stream)
-            host = res.cpu()
-        finally:
-            plan.destroy()
-    out[...] = host.numpy().view(out.dtype)
+            frames.append(resample(v, views[v][s0:s1], s0, inverses[v], z0, n))
+        out[...] = deconvolve(frames)
+    finally:
+        if dev is not None:
+            dev.destroy()
     return z0, out
+
+
+class DeviceShard:
+    """The device half of ``run_shard``: a source buffer the size of one view
+    (only the slab is copied in), the rank's resampled frame and a plan, on
+    the current CUDA device and ``stream``."""
+
+    def __init__(self, src_shape, frame, n, V, kernels, weights, psf_type, bits, pairs_per_batch, iterations,
+                 stream=None):
+        import torch
+
+        from . import api
+        self.api = api
+        self.bits = bits
+        self.iterations = iterations
+        self.dtype = torch.int16 if bits == 16 else torch.uint8
+        self.npdt = np.int16 if bits == 16 else np.uint8
+        d, h, w = src_shape
+        td, th, tw = frame
+        self.src_shape, self.frame, self.n = src_shape, frame, n
+        self.pitch = api.source_pitch(bits, w)
+        self.stream = stream if stream is not None else torch.cuda.current_stream()
+        self.src = torch.zeros((d, h, self.pitch), dtype=self.dtype, device="cuda")
+        self.frame_dev = torch.empty((V, n, th, tw), dtype=self.dtype, device="cuda")
+        self.res = torch.empty((n, th, tw), dtype=self.dtype, device="cuda")
+        self.plan = api.DevicePlan(th, tw, weights, [np.array(k, np.float32) for k in kernels], psf_type, bits=bits,
+                                   pairs_per_batch=pairs_per_batch)
+
+    def resample(self, v, slab, s0, inverse, z0, n):
+        import torch
+        d, h, w = self.src_shape
+        td, th, tw = self.frame
+        with torch.cuda.stream(self.stream):
+            self.src.zero_()
+            if slab.shape[0]:
+                host = torch.from_numpy(np.ascontiguousarray(slab).view(self.npdt)).pin_memory()
+                self.src[s0:s0 + slab.shape[0], :, :w].copy_(host, non_blocking=True)
+            self.api.transform_device(self.src, self.pitch, w, h, d, inverse, tw, th, z0, n, out=self.frame_dev[v],
+                                      stream=self.stream.cuda_stream, bits=self.bits)
+        return self.frame_dev[v]
+
+    def deconvolve(self, frames):
+        import torch
+        with torch.cuda.stream(self.stream):
+            self.plan.run(self.frame_dev, self.res, self.iterations, stream=self.stream.cuda_stream)
+            host = self.res.cpu()
+        return host.numpy().view(np.uint16 if self.bits == 16 else np.uint8)
+
+    def destroy(self):
+        if self.plan is not None:
+            self.plan.destroy()
+            self.plan = None

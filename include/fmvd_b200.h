@@ -64,17 +64,20 @@ int fmvd_b200_plane_stats(const float *d_a, const float *d_b, int nplanes, int H
  * timeout is reported here as an error). */
 int fmvd_b200_plan_check(fmvd_b200_plan *plan);
 void fmvd_b200_plan_destroy(fmvd_b200_plan *plan);
-/* No counterpart in the reference.  fmvd_b200_deconvolve_device without any
- * allocation: the work planes come from one fixed 64 MiB device array of the
- * library, shared by all plans, instead of the plan's own buffers.  For
- * callers that keep many plans alive and cannot spare device memory for each
- * plan's full batch of work planes (create those plans with
- * pairs_per_batch = 1).  Runs as many plane pairs per batch as fit (at most
- * the plan's batch); a padded plane above about 4.19 M points (2048 x 2048)
- * is rejected with an error.  The first call on a device looks up the
- * array's address; make it before any stream capture.  Waits for the stream
- * and reports a timed-out bulk-copy wait itself.  Calls that overlap in time
- * on one device race on the shared array: serialise them. */
+/* No counterpart in the reference.  fmvd_b200_deconvolve_device for callers
+ * that cannot call cudaMalloc where they deconvolve (a framework's memory pool
+ * owns the free device memory, a real-time loop must not take the
+ * allocator's device-wide synchronisation, a plugin runs in another
+ * application's context): the work planes come from one fixed 64 MiB device
+ * array of the library, shared by all plans, instead of the plan's own
+ * buffers (which the plan still holds from its creation).  Runs as many plane
+ * pairs per batch as fit (at most the plan's batch); a padded plane above
+ * about 4.19 M points (2048 x 2048) is rejected with an error.  Call with the
+ * plan's device current.  The first call on a device may load the library's
+ * module there; make it before any stream capture.  Waits for the stream
+ * (also after a failure) and reports a timed-out bulk-copy wait itself.
+ * Calls that overlap in time on one device race on the shared array:
+ * serialise them. */
 int fmvd_b200_deconvolve_device_noalloc(fmvd_b200_plan *plan, const void *d_views, size_t view_stride, void *d_out,
                                         int nplanes, int iterations, float *d_estimate, void *stream);
 

@@ -9,6 +9,8 @@
 // linear filtering, border address mode (0 outside) on all three axes and
 // normalised-float reads.  The per-voxel arithmetic is the reference's:
 // r = M (x, y, z, 1), v = tex3D(r + 0.5), out = (SAMPLE)(v * 2^bits + 0.5).
+// It also restates the reference's weight-mask kernel, so that the reference
+// arm of the benchmark computes its weights without this project's library.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -31,6 +33,35 @@ __global__ void tex_plane_kernel(cudaTextureObject_t tex, S *out, float *raw, in
             raw[idx] = v;
         out[idx] = (S)(v * (1 << BITS) + 0.5);
     }
+}
+
+// Weight mask of target plane z: the reference's create_transformed_mask_kernel
+// (fmvd_transform.cu:19-67) -- 0 where the inverse map leaves the source box,
+// else the product of the cosine ramps 0.5 (1 - cos(pi dist / border)) of the
+// axes nearer than border to an edge, the z distance scaled by zspacing.
+__global__ void mask_plane_kernel(float *out, int z, int w, int h, int d, float zspacing, int tw, int th,
+                                  float border, const float *__restrict__ m)
+{
+    const int x = threadIdx.x + blockIdx.x * blockDim.x;
+    const int y = threadIdx.y + blockIdx.y * blockDim.y;
+    if (x >= tw || y >= th)
+        return;
+    const float r[3] = {m[0] * x + m[1] * y + m[2] * z + m[3], m[4] * x + m[5] * y + m[6] * z + m[7],
+                        m[8] * x + m[9] * y + m[10] * z + m[11]};
+    const int ext[3] = {w, h, d};
+    float v = 1.f;
+    for (int a = 0; a < 3; a++) {
+        if (r[a] < 0 || r[a] >= ext[a]) {
+            v = 0.f;
+            break;
+        }
+        float dist = r[a] < ext[a] / 2 ? r[a] : ext[a] - r[a];
+        if (a == 2)
+            dist *= zspacing;
+        if (dist < border)
+            v *= 0.5f * (1 - cos(dist / border * 3.14159265358979323846f));
+    }
+    out[(size_t)y * tw + x] = v;
 }
 
 // Texture fetch at explicit coordinates (calibration of the filtering model).
@@ -121,6 +152,24 @@ int reftex_transform(int bits, const void *h_vol, int w, int h, int d, int tw, i
                                                  (unsigned short *)h_out, h_raw, ms);
     return run_transform<unsigned char, 8>((const unsigned char *)h_vol, w, h, d, tw, th, td, h_inv,
                                            (unsigned char *)h_out, h_raw, ms);
+}
+
+// Transformed mask of target plane z into h_out (th x tw floats).
+int reftex_mask(const float *h_inv, int z, int w, int h, int d, float zspacing, int tw, int th, float border,
+                float *h_out)
+{
+    float *d_out, *d_m;
+    cudaMalloc(&d_out, (size_t)tw * th * sizeof(float));
+    cudaMalloc(&d_m, 12 * sizeof(float));
+    cudaMemcpy(d_m, h_inv, 12 * sizeof(float), cudaMemcpyHostToDevice);
+    dim3 threads(32, 32);
+    dim3 grid((tw + 31) / 32, (th + 31) / 32);
+    mask_plane_kernel<<<grid, threads>>>(d_out, z, w, h, d, zspacing, tw, th, border, d_m);
+    cudaMemcpy(h_out, d_out, (size_t)tw * th * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(d_out);
+    cudaFree(d_m);
+    cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? 0 : (int)err;
 }
 
 // Hardware texture value at n explicit (x, y, z) coordinates.

@@ -55,10 +55,7 @@ def lib():
 @pytest.fixture(scope="session")
 def ref_lib():
     """The reference library built from the upstream sources (GPU box only)."""
-    import ctypes as C
-    path = os.path.join(REF_DIR, "libfmvd_ref.so")
-    if not os.path.exists(path):
+    from oracle import ref_lib as R
+    if not R.available():
         pytest.skip("reference build not present")
-    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
-    import make_golden
-    return make_golden.load_ref()
+    return R.load_ref()

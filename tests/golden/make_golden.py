@@ -7,11 +7,12 @@ inputs, and writes inputs and outputs as .npz files.  Needs a GPU; run as
 
     python tests/golden/make_golden.py <output dir>
 
+(then copy the .npz files into tests/golden/).
+
 The fixtures pin the CPU oracle (oracle/fmvd_oracle.py) in the CPU tests.
 """
 from __future__ import annotations
 
-import ctypes as C
 import os
 import sys
 
@@ -22,50 +23,7 @@ sys.path.insert(0, ROOT)
 
 from gpu_deconvolution_b200 import synth  # noqa: E402
 
-REF = os.path.join(ROOT, "oracle", "_ref")
-
-
-def load_ref():
-    lib = C.CDLL(os.path.join(REF, "libfmvd_ref.so"))
-    lib.ref_deconvolve.restype = C.c_int
-    lib.ref_deconvolve.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
-                                   C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
-                                   C.c_void_p]
-    lib.ref_last_error.restype = C.c_char_p
-    tex = C.CDLL(os.path.join(REF, "libfmvd_reftex.so"))
-    tex.reftex_transform.restype = C.c_int
-    tex.reftex_transform.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
-                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
-    tex.reftex_probe.restype = C.c_int
-    tex.reftex_probe.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
-    return lib, tex
-
-
-def ref_deconvolve(lib, views, weights, kernels, psf, iterations, nstreams, want_est, max_returned=None):
-    views = np.ascontiguousarray(views)
-    bits = 16 if views.dtype == np.uint16 else 8
-    V, D, H, W = views.shape
-    kH, kW = kernels[0].shape
-    k = np.ascontiguousarray(np.stack(kernels).astype(np.float32))
-    w = np.ascontiguousarray(np.stack(weights).astype(np.float32))
-    mr = max_returned or max(D, nstreams)
-    out = np.zeros((mr, H, W), views.dtype)
-    stats = np.zeros(4, np.int32)
-    est = None
-    if want_est:
-        # room for mr padded planes of up to 1024 x 1024 (the harness packs them)
-        est = np.zeros(mr * 1024 * 1024, np.float32)
-    r = lib.ref_deconvolve(bits, views.ctypes.data, V, D, H, W, w.ctypes.data, k.ctypes.data, kH, kW, psf,
-                           iterations, nstreams, out.ctypes.data, mr, est.ctypes.data if est is not None else None,
-                           stats.ctypes.data)
-    if r != 0:
-        raise RuntimeError(lib.ref_last_error().decode())
-    fh, fw = int(stats[2]), int(stats[3])
-    res = {"out": out[:min(mr, int(stats[1]))], "source_calls": int(stats[0]), "sink_calls": int(stats[1]),
-           "fftH": fh, "fftW": fw, "kernels_normalised": k}
-    if est is not None:
-        res["est"] = est[:mr * fh * fw].reshape(mr, fh, fw)[:min(mr, int(stats[1]))]
-    return res
+from oracle.ref_lib import load_ref, ref_deconvolve  # noqa: E402,F401
 
 
 def rl_cases():
@@ -179,4 +137,6 @@ def main(out_dir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <output dir>")
+    main(sys.argv[1])

@@ -1,10 +1,14 @@
-"""Parity of the B200 deconvolution with the FP64 oracle and with the
-reference's own CUDA build, through the C ABI.
+"""Parity of the B200 deconvolution with the FP64 oracle through the C ABI:
+small planes, every FFT length, all PSF types, 8 and 16 bit, non-square
+kernels, the streaming, file and CLI entry points and the reference's
+call-pattern quirks.  (The oracle itself is pinned to the reference's CUDA
+build by the fixtures of tests/golden/; tests/test_parity_depth_gpu.py runs
+the reference build beside the library at each configuration's depth.)
 
-Tolerances: float estimates within 1e-4 relative L2 of the oracle (and of the
-reference build) after every tested iteration count; sample outputs within
-one unit of the oracle (truncation of values that differ in the last float
-bits), and identical in almost every voxel.
+Tolerances: float estimates within 1e-4 relative L2 of the oracle after every
+tested iteration count; sample outputs within one unit of the oracle
+(truncation of values that differ in the last float bits), and identical in
+almost every voxel.
 """
 import numpy as np
 import pytest

@@ -3,10 +3,11 @@
 CPU tests check the host logic: the plane partition, that the source slab a
 rank uploads holds every plane its target planes weight (planes outside the
 slab are overwritten with a sentinel and the oracle's resampling must not
-change), and a two-rank gloo job whose ranks each resample and deconvolve
-their own planes with the oracle and hand them to rank 0, which must match a
-single-process run of the whole volume.  The GPU test runs the same split
-through the native library.
+change), and gloo jobs of two and three ranks whose ranks each run
+``shard.run_shard`` (plane range, source slabs, result offsets) with the
+oracle standing in for the device resampler and RL, write their planes to one
+file and hand them to rank 0; both must match a single-process run of the
+whole volume.  The GPU test runs the same splits through the native library.
 """
 import os
 import socket
@@ -40,8 +41,10 @@ def test_plane_range_partition():
             assert ranges[0][0] == 0 and ranges[-1][1] == n
             for (a0, a1), (b0, b1) in zip(ranges, ranges[1:]):
                 assert a1 == b0
-            sizes = [b - a for a, b in ranges]
-            assert max(sizes) - min(sizes) <= 1 and min(sizes) >= 0
+            pairs = [(b - a + 1) // 2 for a, b in ranges]
+            assert max(pairs) - min(pairs) <= 1 and min(pairs) >= 0
+            # every share starts at an even plane (plane pairs stay together)
+            assert all(a % 2 == 0 for a, b in ranges if b > a)
     with pytest.raises(ValueError):
         shard.plane_range(4, 2, 2)
 
@@ -87,29 +90,41 @@ def _free_port():
         return s.getsockname()[1]
 
 
+def _oracle_resample(frame):
+    td, th, tw = frame
+
+    def resample(v, slab, s0, inverse, z0, n):
+        # only the slab is known to the rank: the rest of the source is zero
+        vol = np.zeros(_SRC_SHAPE, slab.dtype)
+        vol[s0:s0 + slab.shape[0]] = slab
+        return O.transform_volume(vol, inverse, td, th, tw)[z0:z0 + n]
+    return resample
+
+
+def _oracle_deconvolve(psfs, weights, iterations):
+    return lambda frames: O.deconvolve_volume(np.stack(frames), weights, psfs, 0, iterations)
+
+
+_SRC_SHAPE = small_case()[4]
+
+
 def _gloo_rank(rank, world, port, outfile, result):
     import sys
     sys.path.insert(0, ROOT)
     import torch.distributed as dist
     from gpu_deconvolution_b200 import shard as S
-    from oracle import fmvd_oracle as Or
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         views, mats, psfs, weights, src, frame = small_case()
-        d, h, w = src
-        td, th, tw = frame
-        z0, z1 = S.plane_range(td, rank, world)
-        resampled = []
-        for v in range(len(views)):
-            s0, s1 = S.source_planes(mats[v], w, h, d, tw, th, z0, z1)
-            slab_only = np.zeros_like(views[v])
-            slab_only[s0:s1] = views[v][s0:s1]
-            resampled.append(Or.transform_volume(slab_only, mats[v], td, th, tw)[z0:z1])
-        local = Or.deconvolve_volume(np.stack(resampled), weights, psfs, 0, 3)
+        # the library's host logic (plane range, source slabs, offsets) with
+        # the oracle standing in for the device resampler and RL
+        z0, local = S.run_shard(views, mats, frame, psfs, weights, 3, rank, world,
+                                resample=_oracle_resample(frame), deconvolve=_oracle_deconvolve(psfs, weights, 3))
+        assert (z0, z0 + local.shape[0]) == S.plane_range(frame[0], rank, world)
         S.write_planes(outfile, local, z0)
-        full = S.gather_planes(local, z0, td)
+        full = S.gather_planes(local, z0, frame[0])
         if rank == 0:
             np.save(result, full)
         dist.barrier()
@@ -117,7 +132,10 @@ def _gloo_rank(rank, world, port, outfile, result):
         dist.destroy_process_group()
 
 
-def test_two_rank_gloo_job_matches_single_process():
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_job_matches_single_process(world):
+    """A world-rank gloo job (world 3 splits 20 planes as 8 + 6 + 6) through
+    run_shard's host logic matches one process running the whole volume."""
     import torch.multiprocessing as mp
     views, mats, psfs, weights, src, frame = small_case()
     td, th, tw = frame
@@ -126,7 +144,7 @@ def test_two_rank_gloo_job_matches_single_process():
     with tempfile.TemporaryDirectory() as tmp:
         outfile = os.path.join(tmp, "result.raw")
         result = os.path.join(tmp, "gathered.npy")
-        mp.start_processes(_gloo_rank, args=(2, _free_port(), outfile, result), nprocs=2, join=True,
+        mp.start_processes(_gloo_rank, args=(world, _free_port(), outfile, result), nprocs=world, join=True,
                            start_method="spawn")
         gathered = np.load(result)
         written = np.fromfile(outfile, np.uint16).reshape(td, th, tw)
@@ -135,16 +153,17 @@ def test_two_rank_gloo_job_matches_single_process():
 
 
 @pytest.mark.gpu
-def test_sharded_run_matches_whole_volume_gpu():
-    """Ranks of a 2-way split run one after another on one GPU (they never
-    wait on each other); planes split at an even offset keep their partner
-    plane in the paired FFT, so the assembled volume is bit-identical to the
-    whole-volume run."""
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_run_matches_whole_volume_gpu(world):
+    """Ranks of a split run one after another on one GPU (they never wait on
+    each other); shares start at even planes, so each plane keeps its
+    partner in the paired FFT and the assembled volume is bit-identical to
+    the whole-volume run (world 3: an uneven 8 + 6 + 6 split)."""
     views, mats, psfs, weights, src, frame = small_case()
     td = frame[0]
     _, whole = shard.run_shard(views, mats, frame, psfs, weights, 4, 0, 1)
-    parts = [shard.run_shard(views, mats, frame, psfs, weights, 4, r, 2) for r in range(2)]
-    assert parts[1][0] % 2 == 0
+    parts = [shard.run_shard(views, mats, frame, psfs, weights, 4, r, world) for r in range(world)]
+    assert all(z0 % 2 == 0 for z0, _ in parts)
     assembled = np.concatenate([p for _, p in parts])
     assert assembled.shape[0] == td
     np.testing.assert_array_equal(assembled, whole)

@@ -58,6 +58,31 @@ def test_noalloc_matches_plan_entry_two_calls(pairs):
         plan.destroy()
 
 
+def test_noalloc_several_batches_fewer_pairs_than_plan():
+    """1024 x 1024 padded planes: the shared array holds 3 plane pairs, the
+    plan's batch 8, so 11 planes run as two batches in the array, at a batch
+    size the plan itself never uses."""
+    torch = pytest.importorskip("torch")
+    lib = native.load()
+    H = W = 1000
+    V, D, iters = 2, 11, 2
+    psfs = [synth.gaussian_psf(9, 9, 1.0, 2.0, 90.0 * v) for v in range(V)]
+    weights = [np.full((H, W), 1.0, np.float32) for _ in range(V)]
+    plan = api.DevicePlan(H, W, weights, psfs, 0, bits=16, pairs_per_batch=8)
+    try:
+        assert (plan.fftH, plan.fftW, plan.pairs_per_batch) == (1024, 1024, 8)
+        for call, seed in enumerate((21, 22)):
+            views = _views(torch, V, D, H, W, seed)
+            ref_out, ref_est = _run(lib, "fmvd_b200_deconvolve_device", plan, views, iters, plan.fftH, plan.fftW)
+            out, est = _run(lib, "fmvd_b200_deconvolve_device_noalloc", plan, views, iters, plan.fftH, plan.fftW)
+            # batch size changes only the schedule, so this too is expected to
+            # match bit for bit; same tolerances as above
+            assert rel_l2(est, ref_est) < 1e-6, f"call {call}"
+            assert int(np.abs(out.astype(np.int64) - ref_out.astype(np.int64)).max()) <= 1, f"call {call}"
+    finally:
+        plan.destroy()
+
+
 def test_noalloc_rejects_plane_beyond_array():
     lib = native.load()
     H = W = 2000  # padded plane 2048 x 2048: one plane pair needs 64 MiB of work memory
