@@ -64,9 +64,10 @@ def parse():
     p.add_argument("--small", action="store_true", help="small volume for profiler captures")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--workload", default="transform_rl", choices=["transform_rl", "warmstart", "batched", "planes"],
+    p.add_argument("--workload", default="transform_rl", choices=["transform_rl", "warmstart", "batched", "planes", "large"],
                    help="warmstart: learned warm start vs plain RL-50 (time to the RL-50 result); planes: plain "
-                        "RL throughput per padded plane size (--planes)")
+                        "RL throughput per padded plane size (--planes); large: the large streamed configuration "
+                        "(run with --steps 1 --warmup 1: one step takes tens of seconds)")
     p.add_argument("--planes", default="1400,2048",
                    help="planes workload: comma-separated data plane sizes, each padded by a 31 x 31 kernel "
                         "(63 x 63 from 2000 up): 900 -> 1024, 1400 -> 1536, 2048 -> 2560 FFT planes")
@@ -227,10 +228,11 @@ def barrier(world):
 
 
 # --------------------------------------------------------- CPU baseline
-def cpu_baseline(vols, weights, psfs):
+def cpu_baseline(vols, weights, psfs, iterations=4, label=None):
     """The C/OpenMP port of the per-plane update (oracle/fmvd_cpu.c) on a
-    bounded sample: one plane pair per host thread, 4 iterations, all views,
-    on the same 512 x 512 plane geometry."""
+    bounded sample: one plane pair per host thread (at most 96 planes),
+    ``iterations`` iterations, all views, on the workload's plane geometry.
+    vols: per-view frame planes (D x H x W uint16 arrays)."""
     import ctypes as C
     from oracle import fmvd_oracle as O
     path = os.path.join(ROOT, "oracle", "_build", "libfmvd_cpu.so")
@@ -239,22 +241,24 @@ def cpu_baseline(vols, weights, psfs):
     lib = C.CDLL(path)
     threads = int(lib.fmvdcpu_max_threads())
     planes = min(2 * threads, 96)
-    its = 4
-    H, W = FRAME[1], FRAME[2]
-    sample = np.ascontiguousarray(np.stack([v[:planes, :H, :W] if v.shape[0] >= planes else
-                                            np.resize(v, (planes, H, W)) for v in vols]))
+    nv = len(psfs)
+    H, W = vols[0].shape[1:]
+    kH, kW = psfs[0].shape
+    sample = np.ascontiguousarray(np.stack([v[:planes] if v.shape[0] >= planes else np.resize(v, (planes, H, W))
+                                            for v in vols]))
     k1 = np.stack([O.normalize(p) for p in psfs]).astype(np.float32)
     k2 = np.stack(O.compute_kernel2(psfs, 0)).astype(np.float32)
     w = np.ascontiguousarray(np.stack(weights).astype(np.float32))
     out = np.zeros((planes, H, W), np.uint16)
     P = lambda a: C.c_void_p(a.ctypes.data)
     t0 = time.perf_counter()
-    lib.fmvdcpu_deconvolve(16, P(sample), P(w), P(k1), P(k2), V, planes, H, W, KSIZE, KSIZE, its, P(out), None,
+    lib.fmvdcpu_deconvolve(16, P(sample), P(w), P(k1), P(k2), nv, planes, H, W, kH, kW, iterations, P(out), None,
                            threads)
     dt = time.perf_counter() - t0
-    return {"value": H * W * planes * its / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"C/OpenMP port of the per-plane update, {planes} planes x {its} iterations x {V} views "
-                      f"at 512x512 (1024x1024 padded), {dt:.1f} s"}
+    fh, fw = O.snap_transform_size(H + kH - 1), O.snap_transform_size(W + kW - 1)
+    return {"value": H * W * planes * iterations / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"C/OpenMP port of the per-plane update, {planes} planes x {iterations} iterations x {nv} views "
+                      f"at {H}x{W} ({fh}x{fw} padded), {dt:.1f} s"}
 
 
 # ---------------------------------------------------------------- B200
@@ -394,18 +398,25 @@ def run_e2e(args, vols, mats, psfs, weights, src, frame, world=1):
     h2d = V * d * src[1] * src[2] * 2
     d2h = td * th * tw * 2
 
-    t0 = time.perf_counter()
-    frames = np.stack([api.transform_host(pinned[v], mats[v], tw, th, td) for v in range(V)])
-    ref_api_out = api.deconvolve(frames, weights, [p.copy() for p in psfs], 0, ITERATIONS, nstreams=3)
-    dt_ref_api = time.perf_counter() - t0
-    assert ref_api_out.shape[0] == td
+    # the drop-in path as a C program drives it (C datasource and datasink):
+    # resample every view into host memory, then stream the planes through
+    # fmvd_initialize / deconvolve_planes / destroy_cuda_16 with nstreams 3
+    dts = []
+    for _ in range(2):  # the first run also pages in the host buffers
+        t0 = time.perf_counter()
+        frames = np.stack([api.transform_host(pinned[v], mats[v], tw, th, td) for v in range(V)])
+        ref_api_out = api.deconvolve_c_callbacks(frames, weights, [p.copy() for p in psfs], 0, ITERATIONS,
+                                                 nstreams=3)
+        dts.append(time.perf_counter() - t0)
+        assert ref_api_out.shape[0] == td
+    dt_ref_api = dts[-1]
     return {"value": td * th * tw * ITERATIONS * world / dt, "unit": UNIT, "h2d_bytes_per_step": h2d * world,
             "d2h_bytes_per_step": d2h * world, "ms_per_step": dt * 1e3,
             "api": "fmvd_b200_reconstruct_host (pinned sources in, result to host memory)",
             "reference_style_api": {
                 "value": td * th * tw * ITERATIONS / dt_ref_api, "ms_per_step": dt_ref_api * 1e3, "gpus": 1,
                 "api": "fmvd_b200_transform_host x4 + fmvd_initialize/deconvolve_planes/destroy_cuda_16 "
-                       "(frame through host memory, per-plane callbacks)",
+                       "(frame through host memory, C datasource and datasink, nstreams 3)",
                 "h2d_bytes_per_step": h2d + V * td * th * tw * 2, "d2h_bytes_per_step": V * td * th * tw * 2 + d2h}}
 
 
@@ -599,6 +610,143 @@ def run_batched(args):
                                "kernels 9..41, 25 iterations)"}}), flush=True)
 
 
+# Large streamed configuration: 6 views, u16 2048 x 2048 x 512 each, beads and
+# shells (1e5 beads), rotations about y 60 degrees apart, z spacing 1.5,
+# resampled into a 2048 x 2048 x 768 frame, 63 x 63 PSFs (sigma 2 x 8,
+# rotated per view), 50 RL iterations; FFT plane 2560 x 2560.
+LARGE_V = 6
+LARGE_SRC = (512, 2048, 2048)
+LARGE_FRAME = (768, 2048, 2048)
+LARGE_K = 63
+LARGE_ITERATIONS = 50
+LARGE_ZSCALE = 1.5
+LARGE_BEADS = 100000
+LARGE_NAME = ("large streamed: 6 views u16 2048x2048x512 (z spacing 1.5) in pinned host memory -> 2048x2048x768 "
+              "frame, 50 RL iterations, 63x63 PSFs, FFT plane 2560x2560")
+
+
+def large_workload(seed: int):
+    """Seeded synthetic views of the large configuration, generated on the
+    GPU and kept in pinned host memory (25.8 GB), plus matrices and PSFs."""
+    import torch
+    from gpu_deconvolution_b200 import synth
+    d, h, w = LARGE_SRC
+    gt, g = synth.bead_volume_torch(d, h, w, seed, "cuda", LARGE_BEADS / float(d * h * w))
+    synth.add_shells_torch(gt, 3, seed)
+    psfs = [synth.gaussian_psf(LARGE_K, LARGE_K, 2.0, 8.0, 180.0 * v / LARGE_V) for v in range(LARGE_V)]
+    pinned = []
+    for v in range(LARGE_V):
+        view = synth.blur_noise_torch(gt, [psfs[v]], g)[0]
+        host = torch.empty((d, h, w), dtype=torch.int16, pin_memory=True)
+        host.copy_(view)
+        pinned.append(host)
+        del view
+    del gt
+    torch.cuda.empty_cache()
+    shifts = np.random.default_rng(seed).uniform(-8, 8, (LARGE_V, 3))
+    mats = [synth.rotation_y_inverse(360.0 * v / LARGE_V, LARGE_FRAME, LARGE_SRC, LARGE_ZSCALE, shifts[v])
+            for v in range(LARGE_V)]
+    return pinned, mats, psfs
+
+
+def run_large(args):
+    """The large streamed configuration on one GPU.  'value': sources resident
+    on the device, all views resampled into the whole frame and 50 RL
+    iterations over its 768 planes (CUDA events).  'e2e': the same through
+    fmvd_b200_reconstruct_host with the sources in pinned host memory (upload
+    overlapped with the first resampling, result chunks copied back while the
+    next chunk computes).  One step takes tens of seconds; inputs (77 GB on
+    the device) exceed L2 many times over, so no flush is needed."""
+    import torch
+    from gpu_deconvolution_b200 import api, native
+    lib = native.load()
+    V, (d, h, w), (td, th, tw), IT = LARGE_V, LARGE_SRC, LARGE_FRAME, LARGE_ITERATIONS
+    t0 = time.perf_counter()
+    pinned, mats, psfs = large_workload(4321)
+    t_data = time.perf_counter() - t0
+    weights = []
+    for m in mats:
+        t = torch.zeros((th, tw), dtype=torch.float32, device="cuda")
+        api.mask_device(t, td // 2, w, h, d, LARGE_ZSCALE, tw, th, BORDER, m)
+        weights.append(t.cpu().numpy())
+    plan = api.DevicePlan(th, tw, weights, [p.copy() for p in psfs], 0, bits=16)
+    pitch = api.source_pitch(16, w)
+    stream = torch.cuda.current_stream().cuda_stream
+    src_dev = torch.zeros((V, d, h, pitch), dtype=torch.int16, device="cuda")
+    for v in range(V):
+        src_dev[v, :, :, :w].copy_(pinned[v])
+    frame_dev = torch.zeros((V, td, th, tw), dtype=torch.int16, device="cuda")
+    out_dev = torch.zeros((td, th, tw), dtype=torch.int16, device="cuda")
+
+    def step(ev):
+        ev[0].record()
+        for v in range(V):
+            api.transform_device(src_dev[v], pitch, w, h, d, mats[v], tw, th, 0, td, out=frame_dev[v], stream=stream)
+        ev[1].record()
+        plan.run(frame_dev, out_dev, IT, stream=stream)
+        ev[2].record()
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.warmup + args.steps)]
+    for i in range(args.warmup):
+        step(evs[i])
+    torch.cuda.synchronize()
+    launches0 = lib.fmvd_b200_launch_count()
+    with ClockSampler(0) as clk:
+        for i in range(args.warmup, args.warmup + args.steps):
+            step(evs[i])
+        torch.cuda.synchronize()
+    launches = lib.fmvd_b200_launch_count() - launches0
+    timed = evs[args.warmup:]
+    t_total = sum(e[0].elapsed_time(e[2]) for e in timed) / 1e3
+    t_rl = sum(e[1].elapsed_time(e[2]) for e in timed) / 1e3
+    t_tr = t_total - t_rl
+    frames_cpu = [frame_dev[v, :96].cpu().numpy().view(np.uint16) for v in range(V)] if not args.no_cpu else None
+    del src_dev, frame_dev, out_dev
+    torch.cuda.empty_cache()
+
+    voxel_iters = td * th * tw * IT
+    H, W = plan.fftH, plan.fftW
+    alg = BYTES_PER_PADDED_VOXEL_VIEW_ITER * H * W * td * V * IT * args.steps
+    peak, peak_kind = peak_hbm()
+    tr_bytes = V * (d * h * w * 2 + td * th * tw * 2) * args.steps
+
+    e2e = None
+    if not args.no_e2e:
+        out = np.empty(LARGE_FRAME, np.uint16)
+        rec = api.Reconstructor(plan, V, LARGE_SRC, LARGE_FRAME)
+        try:
+            views_np = [p.numpy().view(np.uint16) for p in pinned]
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rec.run(views_np, mats, IT, out)
+            dt = time.perf_counter() - t0
+        finally:
+            rec.destroy()
+        e2e = {"value": voxel_iters / dt, "unit": UNIT, "ms_per_step": dt * 1e3,
+               "h2d_bytes_per_step": V * d * h * w * 2, "d2h_bytes_per_step": td * th * tw * 2,
+               "api": "fmvd_b200_reconstruct_host (pinned sources in, result to host memory)"}
+    cpu = cpu_baseline(frames_cpu, weights, psfs, iterations=1) if frames_cpu is not None else None
+    plan.destroy()
+    print(json.dumps({
+        "metric": METRIC, "value": voxel_iters * args.steps / t_total, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_total / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": LARGE_NAME, "views": V, "frame": list(LARGE_FRAME), "iterations": IT,
+                   "fft_plane": [H, W], "pairs_per_batch": plan.pairs_per_batch,
+                   "l2": "inputs larger than L2 (77 GB resident on the device)",
+                   "rl_ms_per_step": t_rl / args.steps * 1e3, "transform_ms_per_step": t_tr / args.steps * 1e3,
+                   "data_generation_s": t_data},
+        "roofline": {"bound": "hbm", "achieved": alg / t_rl / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / t_rl / 1e9 / peak, "peak_kind": peak_kind,
+                     "kernel": "fused RL view update (line engine, 2560 x 2560 planes)",
+                     "algorithmic_bytes": "14 B per padded voxel per view per iteration", "traffic": None},
+        "transform": {"ms_per_step": t_tr / args.steps * 1e3, "GB_per_s": tr_bytes / t_tr / 1e9,
+                      "frac_of_hbm": tr_bytes / t_tr / 1e9 / peak,
+                      "algorithmic_bytes": "source read once (2 B/voxel) + frame written once (2 B/voxel)"},
+        "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk.summary(),
+    }), flush=True)
+
+
 def run_planes(args):
     """Plain RL on square planes of the given data sizes (4 views, 10
     iterations, synthetic uint16 views), one JSON line per size: padded
@@ -652,6 +800,8 @@ def main():
         run_batched(args)
     elif args.workload == "planes":
         run_planes(args)
+    elif args.workload == "large":
+        run_large(args)
     else:
         run_b200(args)
 

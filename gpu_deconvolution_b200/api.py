@@ -140,6 +140,34 @@ def deconvolve(views: np.ndarray, weights, kernels, psf_type=0, iterations=10, n
     return res
 
 
+def deconvolve_c_callbacks(views: np.ndarray, weights, kernels, psf_type=0, iterations=10, nstreams=3,
+                           return_stats=False):
+    """``deconvolve`` with the datasource and datasink written in C
+    (lib/libfmvd_host_feed.so): the drop-in streaming API as a C program
+    drives it, without Python in the per-plane callbacks.  16-bit views
+    (V x D x H x W); returns the planes the sink received."""
+    views = np.ascontiguousarray(views, np.uint16)
+    V, D, H, W = views.shape
+    feed = native.load_host_feed()
+    ks = np.ascontiguousarray(np.stack([np.asarray(k, np.float32) for k in kernels]))
+    ws = np.ascontiguousarray(np.stack([np.asarray(w, np.float32) for w in weights]))
+    kH, kW = ks.shape[1:]
+    n_out = max(D, nstreams)
+    out = np.zeros((n_out, H, W), np.uint16)
+    counts = np.zeros(2, np.int32)
+    native.clear_errors()
+    got = feed.fmvd_feed_deconvolve_16(views.ctypes.data, V, D, H, W, ws.ctypes.data, ks.ctypes.data, kH, kW,
+                                       int(psf_type), int(iterations), int(nstreams), out.ctypes.data, n_out,
+                                       counts.ctypes.data)
+    native.check("fmvd_feed_deconvolve_16")
+    if got < 0:
+        raise FmvdError("plan creation failed")
+    res = out[:min(got, n_out)]
+    if return_stats:
+        return res, {"source_calls": int(counts[0]), "sink_calls": int(counts[1])}
+    return res
+
+
 def deconvolve_files(view_paths, out_path, dataW, dataH, dataD, weights, kernels, psf_type=0, iterations=10, bits=16):
     """fmvd_deconvolve_files_cuda_*: raw view files in, raw result file out."""
     lib = native.load()

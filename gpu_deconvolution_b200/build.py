@@ -22,6 +22,7 @@ BUILD = os.path.join(PKG, "_build")
 LIB_DIR = os.path.join(PKG, "lib")
 BIN_DIR = os.path.join(PKG, "bin")
 LIB_NAME = "libNativeSPIMReconstructionCuda.so"
+FEED_NAME = "libfmvd_host_feed.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
@@ -108,6 +109,15 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    # a C caller of the streaming API over host memory (benchmark and tests)
+    feed_src = os.path.join(CSRC, "host_feed.cpp")
+    feed = os.path.join(LIB_DIR, FEED_NAME)
+    if os.path.exists(feed_src) and _stale(feed, [feed_src, lib] + _headers()):
+        cmd = [nvcc()] + NVCC_FLAGS + ["--shared", feed_src, "-o", feed, "-L" + LIB_DIR,
+                                       "-lNativeSPIMReconstructionCuda", "-Xlinker", "-rpath=$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"host feed build failed:\n{r.stdout}\n{r.stderr}")
     cli_src = os.path.join(CSRC, "cli_main.cpp")
     cli = os.path.join(BIN_DIR, "fmvd_deconvolve")
     if os.path.exists(cli_src) and _stale(cli, [cli_src, lib]):

@@ -232,28 +232,66 @@ int fmvd_b200_mask_device(float *d_out, int z, int w, int h, int d, float zspaci
 int fmvd_b200_transform_host(int bits, const void *const *h_planes, int w, int h, int d, int tw, int th, int td,
                              const float *h_inverse, void *h_out)
 {
+    // upload through pinned staging, then resample in chunks of target
+    // planes; each chunk's download to pinned staging and its copy into the
+    // caller's buffer overlap the resampling of the next chunk
     const size_t es = bits == 16 ? 2 : 1;
     const size_t pitch = fmvd::source_pitch(bits, w);
-    void *d_src = nullptr, *d_out = nullptr;
+    const size_t plane = (size_t)tw * th * es;
+    int chunk = (int)(((size_t)32 << 20) / (plane ? plane : 1));
+    chunk = chunk < 1 ? 1 : (chunk > td ? (td > 0 ? td : 1) : chunk);
+    void *d_src = nullptr, *d_out = nullptr, *stage[2] = {nullptr, nullptr};
     int *d_status = nullptr;
-    bool ok = FMVD_CHECK(cudaMalloc(&d_src, pitch * h * d * es)) &&
-              FMVD_CHECK(cudaMalloc(&d_out, (size_t)tw * th * td * es)) &&
-              FMVD_CHECK(cudaMalloc(&d_status, sizeof(int))) && FMVD_CHECK(cudaMemset(d_status, 0, sizeof(int)));
-    for (int z = 0; z < d && ok; z++)
-        ok = FMVD_CHECK(cudaMemcpy2D((char *)d_src + pitch * h * z * es, pitch * es, h_planes[z], w * es, w * es, h,
-                                     cudaMemcpyHostToDevice));
-    ok = ok && fmvd::resample_device(bits, d_src, pitch, w, h, d, tw, th, 0, td, h_inverse, d_out, nullptr, d_status, 0);
-    ok = ok && FMVD_CHECK(cudaMemcpy(h_out, d_out, (size_t)tw * th * td * es, cudaMemcpyDeviceToHost));
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    bool ok = FMVD_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) &&
+              FMVD_CHECK(cudaMalloc(&d_src, pitch * h * d * es)) &&
+              FMVD_CHECK(cudaMalloc(&d_out, 2 * plane * chunk)) && FMVD_CHECK(cudaMalloc(&d_status, sizeof(int))) &&
+              FMVD_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), s));
+    for (int k = 0; k < 2 && ok; k++)
+        ok = FMVD_CHECK(cudaMallocHost(&stage[k], plane * chunk)) &&
+             FMVD_CHECK(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
+    ok = ok && fmvd::upload_planes(h_planes, w, h, d, es, pitch, d_src, s);
+    int pending = -1, pending_z = 0, pending_n = 0;
+    for (int z0 = 0, k = 0; ok && z0 < td; z0 += chunk, k ^= 1) {
+        const int n = td - z0 < chunk ? td - z0 : chunk;
+        char *dk = (char *)d_out + (size_t)k * plane * chunk;
+        ok = fmvd::resample_device(bits, d_src, pitch, w, h, d, tw, th, z0, n, h_inverse, dk, nullptr, d_status, s) &&
+             FMVD_CHECK(cudaMemcpyAsync(stage[k], dk, plane * n, cudaMemcpyDeviceToHost, s)) &&
+             FMVD_CHECK(cudaEventRecord(ev[k], s));
+        if (ok && pending >= 0) {
+            ok = FMVD_CHECK(cudaEventSynchronize(ev[pending]));
+            if (ok)
+                memcpy((char *)h_out + plane * pending_z, stage[pending], plane * pending_n);
+        }
+        pending = k;
+        pending_z = z0;
+        pending_n = n;
+    }
+    if (ok && pending >= 0) {
+        ok = FMVD_CHECK(cudaEventSynchronize(ev[pending]));
+        if (ok)
+            memcpy((char *)h_out + plane * pending_z, stage[pending], plane * pending_n);
+    }
     int status = 0;
+    if (s)
+        cudaStreamSynchronize(s);
     if (ok)
-        cudaMemcpy(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost);
-    if (status) {
+        ok = FMVD_CHECK(cudaMemcpy(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (ok && status) {
         fmvd::report_error("fmvd: a resampler brick load did not complete in time");
         ok = false;
+    }
+    for (int k = 0; k < 2; k++) {
+        cudaFreeHost(stage[k]);
+        if (ev[k])
+            cudaEventDestroy(ev[k]);
     }
     cudaFree(d_src);
     cudaFree(d_out);
     cudaFree(d_status);
+    if (s)
+        cudaStreamDestroy(s);
     return ok ? 0 : 1;
 }
 

@@ -6,9 +6,11 @@
 // (fmvd_deconvolve.impl.cpp:205-300).  Here planes are gathered into batches
 // of 2 * pairs_cap planes (pinned host buffers, two batch slots), copied with
 // one transfer per view and direction, and deconvolved together by the engine.
-// While batch k computes on the device, the host pulls batch k+1 from the
-// datasource and hands batch k-1 to the datasink, so host I/O overlaps the
-// device work; uploads and downloads run on their own streams.
+// Each slot computes on its own stream with its own work planes (the engine's
+// two lanes), so the batches of the two slots also overlap on the device.
+// While batch k computes, the host pulls batch k+1 from the datasource and
+// hands batch k-1 to the datasink, so host I/O overlaps the device work;
+// uploads and downloads run on their own streams.
 #include "fmvd_internal.h"
 
 #include <stdlib.h>
@@ -46,8 +48,10 @@ struct Streamer {
         std::vector<S *> view_ptrs;
         int n = 0;
         cudaEvent_t up = nullptr, done = nullptr, down = nullptr;
+        cudaStream_t comp = nullptr;  // this slot's compute stream
+        Engine lane;                  // the engine with this slot's work planes
     } slot[2];
-    cudaStream_t s_up = nullptr, s_comp = nullptr, s_down = nullptr;
+    cudaStream_t s_up = nullptr, s_down = nullptr;
 
     bool init(Engine *e)
     {
@@ -56,13 +60,23 @@ struct Streamer {
         plane = (size_t)e->dims.dataH * e->dims.dataW;
         const int V = e->dims.V;
         bool ok = FMVD_CHECK(cudaStreamCreateWithFlags(&s_up, cudaStreamNonBlocking)) &&
-                  FMVD_CHECK(cudaStreamCreateWithFlags(&s_comp, cudaStreamNonBlocking)) &&
                   FMVD_CHECK(cudaStreamCreateWithFlags(&s_down, cudaStreamNonBlocking));
         for (int k = 0; k < 2 && ok; k++) {
             Slot &sl = slot[k];
+            sl.lane = *e;
+            if (k == 1 && e->lanes > 1) {
+                sl.lane.C = e->laneC[0];
+                sl.lane.est = e->laneEst[0];
+            }
+            ok = FMVD_CHECK(cudaStreamCreateWithFlags(&sl.comp, cudaStreamNonBlocking));
+            // one lane only: both slots share the work planes, so they share a stream
+            if (ok && k == 1 && e->lanes < 2) {
+                cudaStreamDestroy(sl.comp);
+                sl.comp = slot[0].comp;
+            }
             const size_t in_bytes = sizeof(S) * plane * cap_planes * V;
             const size_t out_bytes = sizeof(S) * plane * cap_planes;
-            ok = FMVD_CHECK(cudaMallocHost(&sl.h_in, in_bytes)) && FMVD_CHECK(cudaMalloc(&sl.d_in, in_bytes)) &&
+            ok = ok && FMVD_CHECK(cudaMallocHost(&sl.h_in, in_bytes)) && FMVD_CHECK(cudaMalloc(&sl.d_in, in_bytes)) &&
                  FMVD_CHECK(cudaMallocHost(&sl.h_out, out_bytes)) && FMVD_CHECK(cudaMalloc(&sl.d_out, out_bytes)) &&
                  FMVD_CHECK(cudaEventCreateWithFlags(&sl.up, cudaEventDisableTiming)) &&
                  FMVD_CHECK(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming)) &&
@@ -88,8 +102,9 @@ struct Streamer {
             if (sl.done) cudaEventDestroy(sl.done);
             if (sl.down) cudaEventDestroy(sl.down);
         }
+        if (slot[0].comp) cudaStreamDestroy(slot[0].comp);
+        if (slot[1].comp && slot[1].comp != slot[0].comp) cudaStreamDestroy(slot[1].comp);
         if (s_up) cudaStreamDestroy(s_up);
-        if (s_comp) cudaStreamDestroy(s_comp);
         if (s_down) cudaStreamDestroy(s_down);
     }
 };
@@ -111,7 +126,7 @@ typename Traits<S>::plan_t *initialize(int dataH, int dataW, const float *const 
         return nullptr;
     }
     Engine *e = engine_create(Traits<S>::bits, dataH, dataW, h_Weights, h_Kernel, kernelH, kernelW, type, nViews,
-                              pairs_cap, 0, 1);
+                              pairs_cap, 0, 2);
     if (!e)
         return nullptr;
     Plan<S> *p = new Plan<S>();
@@ -204,11 +219,11 @@ void deconvolve_planes(const typename Traits<S>::plan_t *plan, int iterations)
                                                 cudaMemcpyHostToDevice, st.s_up)))
                     return;
             FMVD_CHECK(cudaEventRecord(sl.up, st.s_up));
-            FMVD_CHECK(cudaStreamWaitEvent(st.s_comp, sl.up, 0));
-            engine_batch(e, sl.d_in, view_stride, sl.d_out, sl.n, iterations, st.s_comp);
+            FMVD_CHECK(cudaStreamWaitEvent(sl.comp, sl.up, 0));
+            engine_batch(&sl.lane, sl.d_in, view_stride, sl.d_out, sl.n, iterations, sl.comp);
             if (!FMVD_CHECK(cudaGetLastError()))
                 return;
-            FMVD_CHECK(cudaEventRecord(sl.done, st.s_comp));
+            FMVD_CHECK(cudaEventRecord(sl.done, sl.comp));
             FMVD_CHECK(cudaStreamWaitEvent(st.s_down, sl.done, 0));
             FMVD_CHECK(cudaMemcpyAsync(sl.h_out, sl.d_out, sizeof(S) * plane * sl.n, cudaMemcpyDeviceToHost,
                                        st.s_down));

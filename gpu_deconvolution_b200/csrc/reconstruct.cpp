@@ -5,11 +5,12 @@
 // The reference's plugin path moves the resampled frame through the host
 // twice (transform_cuda_* writes it out, fmvd_deconvolve_planes_cuda_* reads
 // it back plane by plane).  Here the host traffic is the source volumes in and
-// the result out: the sources are uploaded once, then target planes are
-// processed in chunks on one stream (resample V views into a device chunk,
-// deconvolve it, write the chunk's samples), while a second stream copies the
-// previous chunk's result to pinned staging and the host thread moves it into
-// the caller's buffer.
+// the result out: the sources are uploaded once (on a copy stream, view by
+// view, the first chunk starting on each view as it lands), then target
+// planes are processed in chunks on one stream (resample V views into a
+// device chunk, deconvolve it, write the chunk's samples), while the copy
+// stream moves the previous chunk's result to pinned staging and the host
+// thread moves it into the caller's buffer.
 #include "fmvd_b200.h"
 #include "fmvd_internal.h"
 #include "transform_kernels.h"
@@ -28,6 +29,7 @@ struct fmvd_b200_reconstructor {
     int *status = nullptr;
     cudaStream_t comp = nullptr, copy = nullptr;
     cudaEvent_t done[2] = {}, copied[2] = {};
+    std::vector<cudaEvent_t> uploaded;  // per view: its source volume is on the device
 };
 
 namespace {
@@ -46,6 +48,9 @@ void release(fmvd_b200_reconstructor *r)
         if (r->copied[i])
             cudaEventDestroy(r->copied[i]);
     }
+    for (cudaEvent_t e : r->uploaded)
+        if (e)
+            cudaEventDestroy(e);
     cudaFree(r->status);
     if (r->comp)
         cudaStreamDestroy(r->comp);
@@ -95,6 +100,9 @@ fmvd_b200_reconstructor *fmvd_b200_reconstructor_create(fmvd_b200_plan *plan, in
              FMVD_CHECK(cudaMallocHost(&r->stage[i], (size_t)chunk * plane)) &&
              FMVD_CHECK(cudaEventCreateWithFlags(&r->done[i], cudaEventDisableTiming)) &&
              FMVD_CHECK(cudaEventCreateWithFlags(&r->copied[i], cudaEventDisableTiming));
+    r->uploaded.assign(views, nullptr);
+    for (int v = 0; v < views && ok; v++)
+        ok = FMVD_CHECK(cudaEventCreateWithFlags(&r->uploaded[v], cudaEventDisableTiming));
     if (!ok) {
         release(r);
         return nullptr;
@@ -113,10 +121,13 @@ int fmvd_b200_reconstruct_host(fmvd_b200_reconstructor *r, const void *const *h_
     const size_t plane = (size_t)r->tw * r->th * es;
     const size_t vol = (size_t)r->d * r->h * r->pitch * es;
     bool ok = FMVD_CHECK(cudaMemsetAsync(r->status, 0, sizeof(int), r->comp));
-    // sources: each view d x h x w contiguous on the host -> pitched device rows
+    // sources: each view d x h x w contiguous on the host -> pitched device
+    // rows, on the copy stream; the first chunk resamples view v as soon as
+    // view v has landed, so the upload of later views overlaps it
     for (int v = 0; v < r->V && ok; v++)
         ok = FMVD_CHECK(cudaMemcpy2DAsync((char *)r->src + v * vol, r->pitch * es, h_views[v], (size_t)r->w * es,
-                                          (size_t)r->w * es, (size_t)r->h * r->d, cudaMemcpyHostToDevice, r->comp));
+                                          (size_t)r->w * es, (size_t)r->h * r->d, cudaMemcpyHostToDevice, r->copy)) &&
+             FMVD_CHECK(cudaEventRecord(r->uploaded[v], r->copy));
     const int nchunks = (r->td + r->chunk - 1) / r->chunk;
     auto planes_of = [&](int k) { return r->td - k * r->chunk < r->chunk ? r->td - k * r->chunk : r->chunk; };
     for (int k = 0; k < nchunks && ok; k++) {
@@ -124,7 +135,8 @@ int fmvd_b200_reconstruct_host(fmvd_b200_reconstructor *r, const void *const *h_
         if (k >= 2)  // the copy of chunk k - 2 has read out[b]
             ok = FMVD_CHECK(cudaStreamWaitEvent(r->comp, r->copied[b], 0));
         for (int v = 0; v < r->V && ok; v++)
-            ok = fmvd::resample_device(r->bits, (const char *)r->src + v * vol, r->pitch, r->w, r->h, r->d, r->tw,
+            ok = (k > 0 || FMVD_CHECK(cudaStreamWaitEvent(r->comp, r->uploaded[v], 0))) &&
+                 fmvd::resample_device(r->bits, (const char *)r->src + v * vol, r->pitch, r->w, r->h, r->d, r->tw,
                                        r->th, z0, n, h_inverses + 12 * v,
                                        (char *)r->frame[b] + (size_t)v * r->chunk * plane, nullptr, r->status,
                                        r->comp);

@@ -359,8 +359,8 @@ size_t source_pitch(int bits, int w)
 // pitched device volume: planes are packed into two pinned staging buffers in
 // turn, each staging buffer's copy to the device running while the host
 // packs the next.
-static bool upload_planes(const void *const *h_planes, int w, int h, int d, size_t es, size_t pitch, void *d_src,
-                          cudaStream_t s)
+bool upload_planes(const void *const *h_planes, int w, int h, int d, size_t es, size_t pitch, void *d_src,
+                   cudaStream_t s)
 {
     const size_t row = (size_t)w * es, plane = row * h;
     int per = (int)(((size_t)32 << 20) / (plane ? plane : 1));

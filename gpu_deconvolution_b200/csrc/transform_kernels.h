@@ -18,6 +18,11 @@ bool resample_device(int bits, const void *d_src, size_t pitch, int w, int h, in
                      const float *h_inverse, void *d_out, float *d_outf, int *d_status, cudaStream_t s);
 void resample_direct(int bits, const void *d_src, size_t pitch, int w, int h, int d, int tw, int th, int z0, int nz,
                      const float *h_inverse, void *d_out, float *d_outf, cudaStream_t s);
+// Upload of d source planes (host pointers into any host memory, w samples
+// per row, h rows) into the pitched device volume d_src through two pinned
+// staging buffers used in turn; returns once the copies have landed.
+bool upload_planes(const void *const *h_planes, int w, int h, int d, size_t es, size_t pitch, void *d_src,
+                   cudaStream_t s);
 // Transformed weight mask of target plane z (tw x th floats).
 bool mask_device(float *d_out, int z, int w, int h, int d, float zspacing, int tw, int th, float border,
                  const float *h_inverse, cudaStream_t s);

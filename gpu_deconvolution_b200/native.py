@@ -14,7 +14,7 @@ import threading
 
 import numpy as np
 
-from .build import LIB_DIR, LIB_NAME
+from .build import FEED_NAME, LIB_DIR, LIB_NAME
 
 _lib = None
 _lock = threading.Lock()
@@ -150,6 +150,27 @@ def load(path: str | None = None):
         lib.setErrorHandler(_record_error, None)
         _lib = lib
         return lib
+
+
+_feed = None
+
+
+def load_host_feed():
+    """The C caller of the streaming API over host memory
+    (lib/libfmvd_host_feed.so, linked against the main library)."""
+    global _feed
+    load()
+    with _lock:
+        if _feed is None:
+            p = os.path.join(LIB_DIR, FEED_NAME)
+            if not os.path.exists(p):
+                raise FmvdError(f"host feed library not built: {p} (run gpu_deconvolution_b200/build.py)")
+            f = C.CDLL(p)
+            f.fmvd_feed_deconvolve_16.restype = c_int
+            f.fmvd_feed_deconvolve_16.argtypes = [c_p, c_int, c_int, c_int, c_int, c_p, c_p, c_int, c_int, c_int,
+                                                  c_int, c_int, c_p, c_int, c_p]
+            _feed = f
+        return _feed
 
 
 def check(context: str = "") -> None:

@@ -157,6 +157,28 @@ def bead_volume_torch(D, H, W, seed, device="cuda", density=5e-5, amp=(500.0, 20
     return x[0, 0] + background, g
 
 
+def add_shells_torch(gt, n_shells: int, seed: int, value: float = 300.0, planes_per_chunk: int = 16):
+    """Adds ``n_shells`` smooth ellipsoidal shells of peak ``value`` to the
+    D x H x W CUDA volume ``gt`` in place (the shells of ``bead_volume``,
+    evaluated a few planes at a time)."""
+    import torch
+    D, H, W = gt.shape
+    rng = np.random.default_rng(seed)
+    dev = gt.device
+    yy = torch.arange(H, device=dev, dtype=torch.float32)[None, :, None]
+    xx = torch.arange(W, device=dev, dtype=torch.float32)[None, None, :]
+    for _ in range(n_shells):
+        c = rng.uniform(0.3, 0.7, 3) * np.array([D, H, W])
+        radii = rng.uniform(0.15, 0.3, 3) * np.array([D, H, W])
+        for z0 in range(0, D, planes_per_chunk):
+            z1 = min(z0 + planes_per_chunk, D)
+            zz = torch.arange(z0, z1, device=dev, dtype=torch.float32)[:, None, None]
+            rho = torch.sqrt(((zz - c[0]) / radii[0]) ** 2 + ((yy - c[1]) / radii[1]) ** 2 +
+                             ((xx - c[2]) / radii[2]) ** 2)
+            gt[z0:z1] += value * torch.exp(-0.5 * ((rho - 1.0) / 0.05) ** 2)
+    return gt
+
+
 def blur_noise_torch(gt, psfs, g, bits: int = 16):
     """V x D x H x W views of ``gt``: per-plane 'same' convolution with each
     PSF, Poisson noise, quantised (int16 holding uint16 bits, or uint8)."""

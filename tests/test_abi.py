@@ -129,3 +129,11 @@ def test_reference_style_cxx_caller_links(tmp_path):
     r = subprocess.run(["g++", str(src), "-o", str(exe), LIB, "-Wl,-rpath," + os.path.dirname(LIB)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_host_feed_library_loads_without_gpu():
+    """The C caller of the streaming API (lib/libfmvd_host_feed.so) loads and
+    resolves its calls into the main library."""
+    from gpu_deconvolution_b200 import native
+    feed = native.load_host_feed()
+    assert feed.fmvd_feed_deconvolve_16 is not None

@@ -162,6 +162,18 @@ def test_streaming_api_matches_device_api():
     assert stats["source_calls"] == 6 and stats["sink_calls"] == 5
 
 
+def test_streaming_c_callbacks_match_device_api():
+    """The streaming API driven by a C datasource and datasink
+    (lib/libfmvd_host_feed.so) gives the device API's planes and the
+    reference's call counts."""
+    views, psfs, weights, _ = synth.plain_rl_views(shape=(13, 40, 44), n_views=3, n_beads=10, ksize=9, seed=16)
+    dev, _ = device_estimates(views, weights, psfs, 0, 3)
+    got, stats = api.deconvolve_c_callbacks(views, weights, [p.copy() for p in psfs], 0, 3, nstreams=3,
+                                            return_stats=True)
+    assert np.array_equal(got, dev)
+    assert stats["source_calls"] == 14 and stats["sink_calls"] == 13
+
+
 def test_streaming_fewer_planes_than_streams():
     """Reference quirk: a source with 1 plane and nstreams = 3 gives 3 sink
     calls and 4 source calls; the first plane is the real result."""
