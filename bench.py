@@ -73,6 +73,10 @@ def parse():
                         "(63 x 63 from 2000 up): 900 -> 1024, 1400 -> 1536, 2048 -> 2560 FFT planes")
     p.add_argument("--pairs-per-batch", type=int, default=0,
                    help="planes workload: plane pairs per batch (0: the library's default)")
+    p.add_argument("--no-warmstart", action="store_true", help="skip the learned warm-start comparison")
+    p.add_argument("--large-train-planes", type=int, default=192,
+                   help="large workload: frame planes whose 512 x 512 crops train the warm-start network")
+    p.add_argument("--large-epochs", type=int, default=8)
     p.add_argument("--train-planes", type=int, default=4000)
     p.add_argument("--epochs", type=int, default=12)
     p.add_argument("--target-iterations", type=int, default=42,
@@ -336,6 +340,16 @@ def run_b200(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         frames = frame_dev[:, :min(96, td)].cpu().numpy().view(np.uint16)
         cpu = cpu_baseline(list(frames), weights, psfs)
+    warm = None
+    if rank == 0 and world == 1 and not args.no_warmstart and not args.small:
+        # the metric's second half: time to the plain RL-50 result, learned
+        # warm start vs plain RL (its own workload, after the timed region)
+        del frame_dev, src_dev, out_dev
+        torch.cuda.empty_cache()
+        try:
+            warm = warmstart_result(args, log=False)
+        except Exception as exc:  # reported in the line, never hides the RL figures
+            warm = {"error": f"{type(exc).__name__}: {exc}"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -360,6 +374,7 @@ def run_b200(args):
             "cpu_baseline": cpu,
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
+            "warmstart": warm,
         }
         print(json.dumps(line), flush=True)
     plan.destroy()
@@ -495,6 +510,10 @@ def unet_flops_per_plane(H, W, V=4, base=32):
 
 
 def run_warmstart(args):
+    print(json.dumps(warmstart_result(args)), flush=True)
+
+
+def warmstart_result(args, log=True):
     """Learned warm start (a 2-D U-Net on the tensor cores) vs plain RL-50 on
     512 x 512 planes of 4 views: train on plain RL-50 targets, tune k so that
     warm start + RL-k is within 1e-2 relative L2 of plain RL-50 on held-out
@@ -517,7 +536,7 @@ def run_warmstart(args):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     hist = WS.train(net, views, targets, epochs=args.epochs, batch=16, lr=1e-3,
-                    log=lambda m: print(m, file=sys.stderr, flush=True))
+                    log=(lambda m: print(m, file=sys.stderr, flush=True)) if log else None)
     e1.record()
     torch.cuda.synchronize()
     t_train = e0.elapsed_time(e1) / 1e3
@@ -554,9 +573,10 @@ def run_warmstart(args):
         "config": {"workload": "learned warm start: 4 views u16 512x512 planes, 17x17 PSFs sigma 1.5x4.0, "
                                "plain RL-50 targets, U-Net 4 levels base 32", "fft_plane": [plan.fftH, plan.fftW]},
     }
-    print(json.dumps(line), flush=True)
     plan.destroy()
     net.destroy()
+    torch.cuda.empty_cache()
+    return line
 
 
 def run_batched(args):
@@ -701,7 +721,14 @@ def run_large(args):
     t_rl = sum(e[1].elapsed_time(e[2]) for e in timed) / 1e3
     t_tr = t_total - t_rl
     frames_cpu = [frame_dev[v, :96].cpu().numpy().view(np.uint16) for v in range(V)] if not args.no_cpu else None
-    del src_dev, frame_dev, out_dev
+    del src_dev
+    warm = None
+    if not args.no_warmstart:
+        try:
+            warm = large_warmstart(args, plan, frame_dev)
+        except Exception as exc:  # reported in the line, never hides the RL figures
+            warm = {"error": f"{type(exc).__name__}: {exc}"}
+    del frame_dev, out_dev
     torch.cuda.empty_cache()
 
     voxel_iters = td * th * tw * IT
@@ -744,7 +771,80 @@ def run_large(args):
                       "frac_of_hbm": tr_bytes / t_tr / 1e9 / peak,
                       "algorithmic_bytes": "source read once (2 B/voxel) + frame written once (2 B/voxel)"},
         "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk.summary(),
+        "warmstart": warm,
     }), flush=True)
+
+
+def large_warmstart(args, plan, frame_dev):
+    """Learned warm start + RL against plain RL-50 on the large configuration's
+    2048 x 2048 planes (6 views, 63 x 63 PSFs, transformed-mask weights).
+
+    The network (6 views + their mean in, BF16 tcgen05 kernels) is trained on
+    512 x 512 crops of registered frame planes with targets = the same crops
+    of the planes' plain RL-50 results; it then runs on whole 2048 x 2048
+    planes (the same parameters in a network sized for them).  k is tuned on
+    held-out planes, and both paths are timed on test planes; training,
+    tuning and test planes are disjoint plane ranges of the frame."""
+    import torch
+    from gpu_deconvolution_b200 import warmstart as WS
+    V, td, th, tw = frame_dev.shape
+    N_RL, TOL, CROP = LARGE_ITERATIONS, 1e-2, 512
+    n_train = args.large_train_planes
+    z_train = 64
+    z_tune, z_test = z_train + n_train + 8, z_train + n_train + 40
+    t0 = time.perf_counter()
+    targets = torch.empty((n_train, th, tw), dtype=torch.float32, device="cuda")
+    for z0 in range(0, n_train, 16):
+        n = min(16, n_train - z0)
+        est, _ = WS.rl_planes(plan, frame_dev[:, z_train + z0:z_train + z0 + n], N_RL)
+        targets[z0:z0 + n] = est
+    # 512 x 512 crops on a 4 x 4 grid of every training plane
+    cv, ct = [], []
+    for y0 in range(0, th, CROP):
+        for x0 in range(0, tw, CROP):
+            cv.append(frame_dev[:, z_train:z_train + n_train, y0:y0 + CROP, x0:x0 + CROP])
+            ct.append(targets[:, y0:y0 + CROP, x0:x0 + CROP])
+    crop_views = torch.cat(cv, dim=1).contiguous()
+    crop_targets = torch.cat(ct, dim=0).contiguous()
+    del cv, ct, targets
+    t_data = time.perf_counter() - t0
+    net = WS.WarmStartNet(CROP, CROP, V, max_batch=16, seed=0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    hist = WS.train(net, crop_views, crop_targets, epochs=args.large_epochs, batch=16, lr=1e-3)
+    e1.record()
+    torch.cuda.synchronize()
+    t_train = e0.elapsed_time(e1) / 1e3
+    n_crops = crop_views.shape[1]
+    del crop_views, crop_targets
+    torch.cuda.empty_cache()
+    full = WS.WarmStartNet(th, tw, V, max_batch=2, seed=0)
+    full.set_params(net.params())
+    net.destroy()
+    tune_views = frame_dev[:, z_tune:z_tune + 8].contiguous()
+    test_views = frame_dev[:, z_test:z_test + 16].contiguous()
+    tune_ref, _ = WS.rl_planes(plan, tune_views, N_RL)
+    tune_ref = tune_ref.contiguous()
+    k, k_errors = WS.tune_k(full, plan, tune_views, tune_ref, TOL,
+                            candidates=tuple(range(0, 13)) + (14, 16, 20, 25, 30, 40))
+    kk = k if k is not None else N_RL
+    t_plain = WS.time_cuda(lambda: WS.rl_planes(plan, test_views, N_RL))
+    t_warm = WS.time_cuda(lambda: WS.warm_deconvolve(full, plan, test_views, kk))
+    t_net = WS.time_cuda(lambda: full.forward(test_views))
+    warm, _ = WS.warm_deconvolve(full, plan, test_views, kk)
+    plain, _ = WS.rl_planes(plan, test_views, N_RL)
+    err = WS.rel_l2_planes(warm.contiguous(), plain.contiguous())
+    full.check()
+    full.destroy()
+    return {"metric": "time to the plain RL-50 result, warm start vs plain", "unit": "ms per 16 planes",
+            "value": t_warm, "plain_rl50_ms": t_plain, "speedup": t_plain / t_warm, "k": k,
+            "rel_l2_vs_rl50": {"max": float(err.max()), "mean": float(err.mean()), "tolerance": TOL},
+            "k_search": {str(a): b for a, b in k_errors.items()}, "network_ms_per_16_planes": t_net,
+            "training": {"planes": n_train, "crops": n_crops, "crop": CROP, "epochs": args.large_epochs,
+                         "seconds": t_train, "loss_per_epoch": hist, "data_seconds": t_data},
+            "planes": {"train": [z_train, z_train + n_train], "tune": [z_tune, z_tune + 8],
+                       "test": [z_test, z_test + 16]},
+            "note": "no PSNR: the frame's ground truth is not resampled"}
 
 
 def run_planes(args):

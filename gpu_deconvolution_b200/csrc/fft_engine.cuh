@@ -133,4 +133,119 @@ struct Dft<16, DIR> {
     }
 };
 
+// ------------------------------------------- forward DFTs of length 3..8
+// SmallDft<R>::run(z): z[k] = sum_n z[n] exp(-2 pi i n k / R), in place, with
+// R-specific short forms for 3, 4, 5 and 8 and a direct form for 6 and 7.
+// cos / sin (2 pi j / R) (mathematical constants)
+constexpr float kC3 = -0.5f, kS3 = 0.86602540378443864676f;
+constexpr float kC5a = 0.30901699437494742410f, kC5b = -0.80901699437494742410f;
+constexpr float kS5a = 0.95105651629515357212f, kS5b = 0.58778525229247312917f;
+// cos / sin (2 pi j / R) for R = 6, 7 (a switch that folds away once j is a
+// compile-time constant after unrolling)
+template <int R>
+__device__ __forceinline__ void unit_root(int j, float &c, float &s)
+{
+    if constexpr (R == 6) {
+        constexpr float h = 0.86602540378443864676f;
+        switch (j) {
+        case 0: c = 1.f; s = 0.f; break;
+        case 1: c = 0.5f; s = h; break;
+        case 2: c = -0.5f; s = h; break;
+        case 3: c = -1.f; s = 0.f; break;
+        case 4: c = -0.5f; s = -h; break;
+        default: c = 0.5f; s = -h; break;
+        }
+    } else {
+        static_assert(R == 7, "direct forms for 6 and 7 only");
+        constexpr float c1 = 0.62348980185873353053f, c2 = -0.22252093395631440429f, c3 = -0.90096886790241912624f;
+        constexpr float s1 = 0.78183148246802980871f, s2 = 0.97492791218182360702f, s3 = 0.43388373911755812048f;
+        switch (j) {
+        case 0: c = 1.f; s = 0.f; break;
+        case 1: c = c1; s = s1; break;
+        case 2: c = c2; s = s2; break;
+        case 3: c = c3; s = s3; break;
+        case 4: c = c3; s = -s3; break;
+        case 5: c = c2; s = -s2; break;
+        default: c = c1; s = -s1; break;
+        }
+    }
+}
+
+// -i * b
+__device__ __forceinline__ float2 cmul_negi(float2 b) { return make_float2(b.y, -b.x); }
+
+template <int R>
+struct SmallDft;
+
+template <>
+struct SmallDft<3> {
+    static __device__ __forceinline__ void run(float2 *z)
+    {
+        const float2 t1 = cadd(z[1], z[2]);
+        const float2 d = csub(z[1], z[2]);
+        const float2 t2 = make_float2(z[0].x + kC3 * t1.x, z[0].y + kC3 * t1.y);
+        const float2 u = cmul_negi(make_float2(kS3 * d.x, kS3 * d.y));
+        z[0] = cadd(z[0], t1);
+        z[1] = cadd(t2, u);
+        z[2] = csub(t2, u);
+    }
+};
+
+template <>
+struct SmallDft<4> {
+    static __device__ __forceinline__ void run(float2 *z) { dft4<-1>(z[0], z[1], z[2], z[3]); }
+};
+
+template <>
+struct SmallDft<5> {
+    static __device__ __forceinline__ void run(float2 *z)
+    {
+        const float2 t1 = cadd(z[1], z[4]), t2 = cadd(z[2], z[3]);
+        const float2 t3 = csub(z[1], z[4]), t4 = csub(z[2], z[3]);
+        const float2 a1 = make_float2(z[0].x + kC5a * t1.x + kC5b * t2.x, z[0].y + kC5a * t1.y + kC5b * t2.y);
+        const float2 a2 = make_float2(z[0].x + kC5b * t1.x + kC5a * t2.x, z[0].y + kC5b * t1.y + kC5a * t2.y);
+        const float2 b1 = make_float2(kS5a * t3.x + kS5b * t4.x, kS5a * t3.y + kS5b * t4.y);
+        const float2 b2 = make_float2(kS5b * t3.x - kS5a * t4.x, kS5b * t3.y - kS5a * t4.y);
+        z[0] = cadd(z[0], cadd(t1, t2));
+        const float2 m1 = cmul_negi(b1), m2 = cmul_negi(b2);
+        z[1] = cadd(a1, m1);
+        z[4] = csub(a1, m1);
+        z[2] = cadd(a2, m2);
+        z[3] = csub(a2, m2);
+    }
+};
+
+template <int R>
+struct DirectDft {
+    static __device__ __forceinline__ void run(float2 *z)
+    {
+        float2 o[R];
+#pragma unroll
+        for (int k = 0; k < R; k++) {
+            float2 acc = z[0];
+#pragma unroll
+            for (int n = 1; n < R; n++) {
+                float c, s;
+                unit_root<R>((n * k) % R, c, s);
+                // z[n] * (cos - i sin)
+                acc.x += z[n].x * c + z[n].y * s;
+                acc.y += z[n].y * c - z[n].x * s;
+            }
+            o[k] = acc;
+        }
+#pragma unroll
+        for (int k = 0; k < R; k++)
+            z[k] = o[k];
+    }
+};
+
+template <>
+struct SmallDft<6> : DirectDft<6> {};
+template <>
+struct SmallDft<7> : DirectDft<7> {};
+template <>
+struct SmallDft<8> {
+    static __device__ __forceinline__ void run(float2 *z) { Dft<8, -1>::run(z); }
+};
+
 } // namespace fmvd

@@ -30,6 +30,7 @@
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <type_traits>
 #include <vector>
 
 namespace fmvd {
@@ -687,13 +688,6 @@ __device__ __forceinline__ void line_twiddle(float2 *v, const float2 *__restrict
     }
 }
 
-// w_R^(r j) (twN: w_N^n with N = R * kLineM)
-template <int R>
-__device__ __forceinline__ float2 line_coefficient(const float2 *__restrict__ twN, int r, int j)
-{
-    return __ldg(twN + ((r * j) % R) * kLineM);
-}
-
 // Row pass for W = R * 512: R warps, two rows per block (half-warp h of warp
 // r is group r of row h).
 // SMEM: the launch bulk-copies each row's weight row (update) or data rows
@@ -736,23 +730,31 @@ __global__ void __launch_bounds__(R * 32, 16 / R) row_pass_r(const RowArgs a)
         }
     }
 
-    // the sum over the row's R groups: v[m] = sum_j (group j's v[m]) w_R^(r j)
-    const auto line_sum = [&](float2 *v) {
+    // the radix-R step across the row's R groups, v[m] <- sum_j (group j's
+    // v[m]) w_R^(r j): every group puts its sub-line in its buffer (position
+    // n1), then each half-warp of the row takes blocks of 16 positions n1
+    // (block b = r, r + R, ...) and runs the R-point DFT over the R buffers
+    // in place, and every group reads its own buffer back
+    const auto line_dft = [&](float2 *v) {
 #pragma unroll
         for (int m = 0; m < E; m++)
             buf[t + T * m] = v[m];
         __syncthreads();
+#pragma unroll 1
+        for (int b = r; b < kLineM / 16; b += R) {
+            float2 z[R];
 #pragma unroll
-        for (int m = 0; m < E; m++)
-            v[m] = lbuf[t + T * m];
+            for (int q = 0; q < R; q++)
+                z[q] = lbuf[q * PF2 + 16 * b + t];
+            SmallDft<R>::run(z);
 #pragma unroll
-        for (int j = 1; j < R; j++) {
-            const float2 cj = line_coefficient<R>(a.twN, r, j);
-#pragma unroll
-            for (int m = 0; m < E; m++)
-                v[m] = cadd(v[m], cmul(lbuf[j * PF2 + t + T * m], cj));
+            for (int q = 0; q < R; q++)
+                lbuf[q * PF2 + 16 * b + t] = z[q];
         }
         __syncthreads();
+#pragma unroll
+        for (int m = 0; m < E; m++)
+            v[m] = buf[t + T * m];
     };
 
     // pass 0: frequency -> space (the inverse as conj(forward(conj))) and
@@ -775,7 +777,7 @@ __global__ void __launch_bounds__(R * 32, 16 / R) row_pass_r(const RowArgs a)
 #pragma unroll 1
     for (int pass = MODE == ROW_INIT ? 1 : 0; pass < 2; pass++) {
         if (pass == 1) {
-            line_sum(v);
+            line_dft(v);
             line_twiddle(v, a.twN, r, t);
         }
         WF::template run_padded<-1>(v, a.tw, buf, t);
@@ -793,7 +795,7 @@ __global__ void __launch_bounds__(R * 32, 16 / R) row_pass_r(const RowArgs a)
             prefetch_l1((const char *)(t < 8 ? work.src0 : work.src1) + (size_t)sx * (BITS == 8 ? 1 : 2));
         }
         line_twiddle(v, a.twN, r, t);
-        line_sum(v);
+        line_dft(v);
         if (staged) {
             if (!mbar_wait(&sbar[h], 0)) {
                 // the copy did not land in time: flag it (the host reports the
@@ -887,23 +889,23 @@ __global__ void __launch_bounds__(R * 32, 16 / R) col_pass_r(const ColArgs a)
     const uint32_t seg = base + 8192u * r;          // this group's sub-line
     const uint32_t wbase = seg | q, rbase = (seg + 256u * t) | q;
 
-    // v[m] = sum_j (row 512 j + t + 16 m of this column) w_R^(r j)
-    const auto column_sum = [&](float2 *v) {
+    // The radix-R step of both columns in place in the tile: each half-warp
+    // takes blocks of 16 positions n1 of its column (block b = r, r + R, ...)
+    // and runs the R-point DFT over the rows 512 q + n1 (q < R); with CONJ the
+    // results are stored conjugated.  The tile address of row 512 q + 16 b + t
+    // of this column is col + 8192 q + 256 b.
+    const auto column_dft = [&](auto conj_out) {
+#pragma unroll 1
+        for (int b = r; b < kLineM / 16; b += R) {
+            float2 z[R];
 #pragma unroll
-        for (int m = 0; m < E; m++)
-            v[m] = lds2(col + 256u * m);
+            for (int q = 0; q < R; q++)
+                z[q] = lds2(col + 8192u * q + 256u * b);
+            SmallDft<R>::run(z);
 #pragma unroll
-        for (int j = 1; j < R; j++) {
-            const float2 cj = line_coefficient<R>(a.twN, r, j);
-#pragma unroll
-            for (int m0 = 0; m0 < E; m0 += 8) {
-                asm volatile("" ::: "memory");  // bounds the loads in flight
-#pragma unroll
-                for (int m = m0; m < m0 + 8; m++)
-                    v[m] = cadd(v[m], cmul(lds2(col + 8192u * j + 256u * m), cj));
-            }
+            for (int q = 0; q < R; q++)
+                sts2(col + 8192u * q + 256u * b, decltype(conj_out)::value ? make_float2(z[q].x, -z[q].y) : z[q]);
         }
-        asm volatile("" ::: "memory");
     };
 
     float2 v[E];
@@ -915,8 +917,12 @@ __global__ void __launch_bounds__(R * 32, 16 / R) col_pass_r(const ColArgs a)
 #pragma unroll 1
     for (int pass = 0; pass < 2; pass++) {
         if (pass == 0) {
-            column_sum(v);
-            __syncthreads();  // every group has read the column before transposes overwrite it
+            column_dft(std::false_type());
+            __syncthreads();  // every block of positions has its radix-R step
+#pragma unroll
+            for (int m = 0; m < E; m++)
+                v[m] = lds2(col + 8192u * r + 256u * m);  // row 512 r + t + 16 m: this group's sub-line
+            __syncwarp();  // read before this warp's transposes overwrite its segment
             line_twiddle(v, a.twN, r, t);
         }
         col_fft_512<-1>(v, a.tw, wbase, rbase, t);
@@ -938,11 +944,7 @@ __global__ void __launch_bounds__(R * 32, 16 / R) col_pass_r(const ColArgs a)
     for (int m = 0; m < E; m++)
         sts2(seg + q + 256u * m, v[m]);  // row 512 r + t + 16 m
     __syncthreads();
-    column_sum(v);
-    __syncthreads();
-#pragma unroll
-    for (int m = 0; m < E; m++)
-        sts2(seg + q + 256u * m, make_float2(v[m].x, -v[m].y));
+    column_dft(std::true_type());
     __syncthreads();
 #pragma unroll 4
     for (int i = 0; i < H / NT; i++) {

@@ -4,12 +4,14 @@
 // which binds the source to a 3-D texture and fetches every target voxel with
 // hardware trilinear filtering.  Here the source lives in plain device memory
 // (rows padded to 16 bytes) described by a 3-D TMA tensor map.  Each CTA
-// resamples a 32 x 8 tile of one target plane: since the map is affine, every
-// tile's source footprint has the same shape, so the host sizes one box that
-// covers it (with slack for rounding), one thread issues a single
-// cp.async.bulk.tensor load of that brick into shared memory (out-of-volume
-// texels arrive as zeros, the texture's border colour), and the threads
-// interpolate from shared memory.  The interpolation follows the texture
+// resamples a 32 x 8 tile of a stack of up to 8 consecutive target planes:
+// since the map is affine, every stack's source footprint has the same shape,
+// so the host sizes one box that covers it (with slack for rounding), one
+// thread issues a single cp.async.bulk.tensor load of that brick into shared
+// memory (out-of-volume texels arrive as zeros, the texture's border colour),
+// and the threads interpolate every plane of the stack from shared memory.
+// Consecutive target planes sample overlapping source footprints, so one
+// brick per stack moves a fraction of the bytes of one brick per plane.  The interpolation follows the texture
 // unit's linear filter: texel centres at i + 0.5, weights held with 8
 // fractional bits, values normalised by 2^bits - 1; output quantised as the
 // reference does, (sample)(v * 2^bits + 0.5) through a 32-bit integer.
@@ -80,23 +82,25 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)_
 template <typename S, int BITS>
 __global__ void __launch_bounds__(TX *TY) resample_tma(const __grid_constant__ CUtensorMap tmap,
                                                        const S *__restrict__ src, int w, int h, int d, size_t pitch,
-                                                       int tw, int th, int z0, const Mat M, int bx, int by, int bz,
-                                                       S *__restrict__ out, float *__restrict__ outf,
+                                                       int tw, int th, int z0, int nz, int kz, const Mat M, int bx,
+                                                       int by, int bz, S *__restrict__ out, float *__restrict__ outf,
                                                        int *__restrict__ status)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar;
     S *brick = reinterpret_cast<S *>(smem_raw);
     constexpr int XALIGN = 16 / sizeof(S);
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z = z0 + blockIdx.z;
+    // this CTA: a TX x TY tile of the kz target planes zb .. zb + kz - 1
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, zb = z0 + blockIdx.z * kz;
+    const int zn = min(kz, z0 + nz - zb);
     const int tid = threadIdx.x;
 
-    // brick origin: minimum over the tile corners, one texel of slack
+    // brick origin: minimum over the corners of the tile stack, one texel of slack
     float mn[3] = {3.4e38f, 3.4e38f, 3.4e38f};
 #pragma unroll
-    for (int c = 0; c < 4; c++) {
+    for (int c = 0; c < 8; c++) {
         float r[3];
-        apply(M, x0 + (c & 1) * (TX - 1), y0 + (c >> 1) * (TY - 1), z, r[0], r[1], r[2]);
+        apply(M, x0 + (c & 1) * (TX - 1), y0 + ((c >> 1) & 1) * (TY - 1), zb + (c >> 2) * (zn - 1), r[0], r[1], r[2]);
 #pragma unroll
         for (int k = 0; k < 3; k++)
             mn[k] = fminf(mn[k], r[k]);
@@ -139,7 +143,12 @@ __global__ void __launch_bounds__(TX *TY) resample_tma(const __grid_constant__ C
         atomicExch(status, 1);
 
     const int x = x0 + (tid % TX), y = y0 + (tid / TX);
-    if (x < tw && y < th) {
+    if (x >= tw || y >= th)
+        return;
+    const float inv = 1.0f / (float)((1 << BITS) - 1);
+#pragma unroll 2
+    for (int k = 0; k < zn; k++) {
+        const int z = zb + k;
         float rx, ry, rz;
         apply(M, x, y, z, rx, ry, rz);
         int ix, iy, iz;
@@ -147,13 +156,13 @@ __global__ void __launch_bounds__(TX *TY) resample_tma(const __grid_constant__ C
         tex_axis(rx, ix, ax);
         tex_axis(ry, iy, ay);
         tex_axis(rz, iz, az);
-        const float inv = 1.0f / (float)((1 << BITS) - 1);
         const int lx = ix - ox, ly = iy - oy, lz = iz - oz;
         float t[8];
         if (have_brick && lx >= 0 && lx + 1 < bx && ly >= 0 && ly + 1 < by && lz >= 0 && lz + 1 < bz) {
+            const S *b0 = brick + (lz * by + ly) * bx + lx;
 #pragma unroll
             for (int c = 0; c < 8; c++)
-                t[c] = to_sample_float(brick[((lz + (c >> 2)) * by + (ly + ((c >> 1) & 1))) * bx + lx + (c & 1)], inv);
+                t[c] = to_sample_float(b0[((c >> 2) * by + ((c >> 1) & 1)) * bx + (c & 1)], inv);
         } else {
 #pragma unroll
             for (int c = 0; c < 8; c++) {
@@ -165,7 +174,7 @@ __global__ void __launch_bounds__(TX *TY) resample_tma(const __grid_constant__ C
         const float bx0 = 1.f - ax, by0 = 1.f - ay, bz0 = 1.f - az;
         const float v = bz0 * (by0 * (bx0 * t[0] + ax * t[1]) + ay * (bx0 * t[2] + ax * t[3])) +
                         az * (by0 * (bx0 * t[4] + ax * t[5]) + ay * (bx0 * t[6] + ax * t[7]));
-        const size_t oi = ((size_t)blockIdx.z * th + y) * tw + x;
+        const size_t oi = ((size_t)(z - z0) * th + y) * tw + x;
         if (out)
             out[oi] = quantise<S, BITS>(v);
         if (outf)
@@ -231,16 +240,27 @@ bool resample_device(int bits, const void *d_src, size_t pitch, int w, int h, in
     Mat M;
     memcpy(M.m, h_inverse, sizeof(M.m));
     const int xalign = (int)(16 / es);
-    // box covering one tile's footprint: extent + 2 texels for the filter and
-    // slack, plus the alignment of the x origin
-    int box[3];
-    for (int a = 0; a < 3; a++) {
-        const float ext = fabsf(M.m[4 * a]) * (TX - 1) + fabsf(M.m[4 * a + 1]) * (TY - 1);
-        box[a] = ceil_i(ext) + 4;
+    // box covering the footprint of a stack of kz tiles: extent + 2 texels
+    // for the filter and slack, plus the alignment of the x origin; kz is the
+    // deepest stack (8, 4, 2 or 1 target planes) whose box fits
+    int box[3] = {0, 0, 0};
+    int kz = 8;
+    size_t smem = 0;
+    bool boxes_ok = false;
+    for (; kz >= 1; kz /= 2) {
+        for (int a = 0; a < 3; a++) {
+            const float ext = fabsf(M.m[4 * a]) * (TX - 1) + fabsf(M.m[4 * a + 1]) * (TY - 1) +
+                              fabsf(M.m[4 * a + 2]) * (kz - 1);
+            box[a] = ceil_i(ext) + 4;
+        }
+        box[0] = ((box[0] + xalign - 1 + xalign - 1) / xalign) * xalign;
+        smem = (size_t)box[0] * box[1] * box[2] * es;
+        boxes_ok = box[0] <= 256 && box[1] <= 256 && box[2] <= 256 && smem <= 96 * 1024;
+        if (boxes_ok)
+            break;
     }
-    box[0] = ((box[0] + xalign - 1 + xalign - 1) / xalign) * xalign;
-    const size_t smem = (size_t)box[0] * box[1] * box[2] * es;
-    const bool boxes_ok = box[0] <= 256 && box[1] <= 256 && box[2] <= 256 && smem <= 96 * 1024;
+    if (kz < 1)
+        kz = 1;
 
     CUtensorMap tmap;
     memset(&tmap, 0, sizeof(tmap));
@@ -260,15 +280,15 @@ bool resample_device(int bits, const void *d_src, size_t pitch, int w, int h, in
         // no brick fits (extreme scaling): every voxel takes the direct path
         box[0] = box[1] = box[2] = 0;
     }
-    dim3 grid((tw + TX - 1) / TX, (th + TY - 1) / TY, nz);
+    dim3 grid((tw + TX - 1) / TX, (th + TY - 1) / TY, (nz + kz - 1) / kz);
     const size_t shm = use_tma ? smem : 0;
     if (bits == 16) {
         auto k = resample_tma<unsigned short, 16>;
         if (shm > 48 * 1024)
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
         if (use_tma) {
-            k<<<grid, TX * TY, shm, s>>>(tmap, (const unsigned short *)d_src, w, h, d, pitch, tw, th, z0, M, box[0],
-                                         box[1], box[2], (unsigned short *)d_out, d_outf, d_status);
+            k<<<grid, TX * TY, shm, s>>>(tmap, (const unsigned short *)d_src, w, h, d, pitch, tw, th, z0, nz, kz, M,
+                                         box[0], box[1], box[2], (unsigned short *)d_out, d_outf, d_status);
             rl_count_launch(1);
         } else {
             resample_direct(bits, d_src, pitch, w, h, d, tw, th, z0, nz, h_inverse, d_out, d_outf, s);
@@ -278,8 +298,8 @@ bool resample_device(int bits, const void *d_src, size_t pitch, int w, int h, in
         if (shm > 48 * 1024)
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
         if (use_tma) {
-            k<<<grid, TX * TY, shm, s>>>(tmap, (const unsigned char *)d_src, w, h, d, pitch, tw, th, z0, M, box[0],
-                                         box[1], box[2], (unsigned char *)d_out, d_outf, d_status);
+            k<<<grid, TX * TY, shm, s>>>(tmap, (const unsigned char *)d_src, w, h, d, pitch, tw, th, z0, nz, kz, M,
+                                         box[0], box[1], box[2], (unsigned char *)d_out, d_outf, d_status);
             rl_count_launch(1);
         } else {
             resample_direct(bits, d_src, pitch, w, h, d, tw, th, z0, nz, h_inverse, d_out, d_outf, s);
