@@ -191,14 +191,20 @@ def peak_hbm():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """Per view-update DRAM bytes of the RL passes from the committed ncu
-    summary, if one exists."""
-    try:
-        with open(os.path.join(ROOT, "profiles", "rl_passes_traffic.json")) as f:
-            return json.load(f)
-    except Exception:
-        return None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the four
+# passes of one view update of a 6-plane batch of 1024 x 1024 planes, per
+# padded voxel, from one ncu capture of this workload's small case:
+#   ncu --set full --cache-control none --clock-control none \
+#       -k regex:"row_pass_w|col_pass_w" -s 40 -c 4 \
+#       python bench.py --small --steps 1 --warmup 1 --no-e2e --no-cpu
+# (22.1 MB per view update; the batch's work planes stay in L2).
+DRAM_BYTES_PER_PADDED_VOXEL_VIEW_UPDATE = 3.52
+# Thread instructions of the same four passes per padded voxel (the same
+# capture's smsp__inst_executed.sum x 32 / padded voxels: 38.62 M warp
+# instructions per view update of the 6-plane batch).  With one warp
+# instruction per SM sub-partition per cycle (148 SMs x 4 x 32 lanes x clock)
+# this gives the issue-bound ceiling of the passes.
+THREAD_INSTR_PER_PADDED_VOXEL_VIEW_UPDATE = 196.3
 
 
 def dist_setup(n):
@@ -323,15 +329,12 @@ def run_b200(args):
     alg_bytes = BYTES_PER_PADDED_VOXEL_VIEW_ITER * H * W * td * V * ITERATIONS * args.steps
     achieved = alg_bytes / t_rl / 1e9
     peak, peak_kind = peak_hbm()
-    traffic = profiled_traffic()
     # one unit of the roofline = one view update of one batch of plane pairs
     # (the four passes row divide, column K^, row update, column K)
     batch_planes = 2 * plan.pairs_per_batch
     n_updates = -(-td // batch_planes) * V * ITERATIONS * args.steps
     alg_per_update = BYTES_PER_PADDED_VOXEL_VIEW_ITER * H * W * batch_planes
-    traffic_per_update = None
-    if traffic and "bytes_per_view_update_per_padded_voxel" in traffic:
-        traffic_per_update = traffic["bytes_per_view_update_per_padded_voxel"] * H * W * batch_planes
+    traffic_per_update = DRAM_BYTES_PER_PADDED_VOXEL_VIEW_UPDATE * H * W * batch_planes
 
     e2e = None
     if not args.no_e2e:
@@ -369,13 +372,24 @@ def run_b200(args):
                          "update_ms": t_rl / n_updates * 1e3,
                          "algorithmic_bytes": "14 B per padded voxel per view per iteration",
                          "traffic": traffic_per_update,
-                         "traffic_source": (traffic or {}).get("source")},
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the four passes of "
+                                           "one view update, small case of this workload (same batch shape)"},
             "e2e": e2e,
             "cpu_baseline": cpu,
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "warmstart": warm,
         }
+        clk_sum = line["clocks"]
+        mhz = clk_sum.get("sm_mhz") or 1965.0
+        issue_rate = 148 * 4 * 32 * mhz * 1e6            # thread instructions per second
+        ceiling = issue_rate / THREAD_INSTR_PER_PADDED_VOXEL_VIEW_UPDATE   # padded voxel-view-updates/s
+        rate = alg_bytes / BYTES_PER_PADDED_VOXEL_VIEW_ITER / t_rl
+        line["roofline"]["issue_ceiling"] = {
+            "padded_voxel_view_updates_per_s": ceiling, "achieved": rate, "frac": rate / ceiling,
+            "as_hbm_frac": ceiling * BYTES_PER_PADDED_VOXEL_VIEW_ITER / 1e9 / peak,
+            "model": f"{THREAD_INSTR_PER_PADDED_VOXEL_VIEW_UPDATE} thread instructions per padded voxel per view "
+                     f"update (ncu) at one warp instruction per SM sub-partition per cycle, {mhz:.0f} MHz"}
         print(json.dumps(line), flush=True)
     plan.destroy()
     if world > 1:

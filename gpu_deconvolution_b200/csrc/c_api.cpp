@@ -234,23 +234,25 @@ int fmvd_b200_transform_host(int bits, const void *const *h_planes, int w, int h
 {
     // upload through pinned staging, then resample in chunks of target
     // planes; each chunk's download to pinned staging and its copy into the
-    // caller's buffer overlap the resampling of the next chunk
+    // caller's buffer overlap the resampling of the next chunk (the staging
+    // buffers are kept from call to call)
+    auto lock = fmvd::staging_lock();
     const size_t es = bits == 16 ? 2 : 1;
     const size_t pitch = fmvd::source_pitch(bits, w);
     const size_t plane = (size_t)tw * th * es;
-    int chunk = (int)(((size_t)32 << 20) / (plane ? plane : 1));
+    int chunk = (int)(((size_t)16 << 20) / (plane ? plane : 1));
     chunk = chunk < 1 ? 1 : (chunk > td ? (td > 0 ? td : 1) : chunk);
-    void *d_src = nullptr, *d_out = nullptr, *stage[2] = {nullptr, nullptr};
+    void *d_src = nullptr, *d_out = nullptr;
+    void *stage[2] = {fmvd::staging_buffer(2, plane * chunk), fmvd::staging_buffer(3, plane * chunk)};
     int *d_status = nullptr;
     cudaStream_t s = nullptr;
     cudaEvent_t ev[2] = {nullptr, nullptr};
-    bool ok = FMVD_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) &&
+    bool ok = stage[0] && stage[1] && FMVD_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) &&
               FMVD_CHECK(cudaMalloc(&d_src, pitch * h * d * es)) &&
               FMVD_CHECK(cudaMalloc(&d_out, 2 * plane * chunk)) && FMVD_CHECK(cudaMalloc(&d_status, sizeof(int))) &&
               FMVD_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), s));
     for (int k = 0; k < 2 && ok; k++)
-        ok = FMVD_CHECK(cudaMallocHost(&stage[k], plane * chunk)) &&
-             FMVD_CHECK(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
+        ok = FMVD_CHECK(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
     ok = ok && fmvd::upload_planes(h_planes, w, h, d, es, pitch, d_src, s);
     int pending = -1, pending_z = 0, pending_n = 0;
     for (int z0 = 0, k = 0; ok && z0 < td; z0 += chunk, k ^= 1) {
@@ -262,7 +264,7 @@ int fmvd_b200_transform_host(int bits, const void *const *h_planes, int w, int h
         if (ok && pending >= 0) {
             ok = FMVD_CHECK(cudaEventSynchronize(ev[pending]));
             if (ok)
-                memcpy((char *)h_out + plane * pending_z, stage[pending], plane * pending_n);
+                fmvd::host_copy((char *)h_out + plane * pending_z, stage[pending], plane * pending_n);
         }
         pending = k;
         pending_z = z0;
@@ -271,7 +273,7 @@ int fmvd_b200_transform_host(int bits, const void *const *h_planes, int w, int h
     if (ok && pending >= 0) {
         ok = FMVD_CHECK(cudaEventSynchronize(ev[pending]));
         if (ok)
-            memcpy((char *)h_out + plane * pending_z, stage[pending], plane * pending_n);
+            fmvd::host_copy((char *)h_out + plane * pending_z, stage[pending], plane * pending_n);
     }
     int status = 0;
     if (s)
@@ -282,11 +284,9 @@ int fmvd_b200_transform_host(int bits, const void *const *h_planes, int w, int h
         fmvd::report_error("fmvd: a resampler brick load did not complete in time");
         ok = false;
     }
-    for (int k = 0; k < 2; k++) {
-        cudaFreeHost(stage[k]);
+    for (int k = 0; k < 2; k++)
         if (ev[k])
             cudaEventDestroy(ev[k]);
-    }
     cudaFree(d_src);
     cudaFree(d_out);
     cudaFree(d_status);

@@ -4,13 +4,13 @@
 // The reference streams one plane per CUDA stream slot through a ring of
 // nstreams slots, 8 launches per view and iteration
 // (fmvd_deconvolve.impl.cpp:205-300).  Here planes are gathered into batches
-// of 2 * pairs_cap planes (pinned host buffers, two batch slots), copied with
-// one transfer per view and direction, and deconvolved together by the engine.
-// Each slot computes on its own stream with its own work planes (the engine's
-// two lanes), so the batches of the two slots also overlap on the device.
-// While batch k computes, the host pulls batch k+1 from the datasource and
-// hands batch k-1 to the datasink, so host I/O overlaps the device work;
-// uploads and downloads run on their own streams.
+// of 2 * pairs_cap planes (pinned host buffers, three batch slots), copied
+// with one transfer per view and direction, and deconvolved together by the
+// engine.  Batches alternate between the engine's two lanes (work planes and
+// stream each), so consecutive batches also overlap on the device.  While
+// batches compute, the host hands the oldest finished batch to the datasink
+// and pulls the next one from the datasource into its slot, so host I/O
+// overlaps the device work; uploads and downloads run on their own streams.
 #include "fmvd_internal.h"
 
 #include <stdlib.h>
@@ -40,17 +40,22 @@ struct Traits<unsigned char> {
 
 template <typename S>
 struct Streamer {
+    // Three batch slots over the engine's two lanes: batch b fills slot
+    // b % 3 and computes on lane b % 2, so while the host fills one slot the
+    // two other batches can be computing on both lanes.
+    static constexpr int kSlots = 3;
     Engine *eng = nullptr;
     int cap_planes = 0;
     size_t plane = 0;
     struct Slot {
         S *h_in = nullptr, *d_in = nullptr, *h_out = nullptr, *d_out = nullptr;
         std::vector<S *> view_ptrs;
-        int n = 0;
+        int n = 0;       // planes of the batch held (0: free)
         cudaEvent_t up = nullptr, done = nullptr, down = nullptr;
-        cudaStream_t comp = nullptr;  // this slot's compute stream
-        Engine lane;                  // the engine with this slot's work planes
-    } slot[2];
+    } slot[kSlots];
+    Engine lane[2];              // the engine with each lane's work planes
+    cudaStream_t comp[2] = {nullptr, nullptr};
+    int nlanes = 1;
     cudaStream_t s_up = nullptr, s_down = nullptr;
 
     bool init(Engine *e)
@@ -59,24 +64,21 @@ struct Streamer {
         cap_planes = 2 * e->pairs_cap;
         plane = (size_t)e->dims.dataH * e->dims.dataW;
         const int V = e->dims.V;
+        nlanes = e->lanes > 1 ? 2 : 1;
+        lane[0] = lane[1] = *e;
+        if (nlanes > 1) {
+            lane[1].C = e->laneC[0];
+            lane[1].est = e->laneEst[0];
+        }
         bool ok = FMVD_CHECK(cudaStreamCreateWithFlags(&s_up, cudaStreamNonBlocking)) &&
                   FMVD_CHECK(cudaStreamCreateWithFlags(&s_down, cudaStreamNonBlocking));
-        for (int k = 0; k < 2 && ok; k++) {
+        for (int l = 0; l < nlanes && ok; l++)
+            ok = FMVD_CHECK(cudaStreamCreateWithFlags(&comp[l], cudaStreamNonBlocking));
+        for (int k = 0; k < kSlots && ok; k++) {
             Slot &sl = slot[k];
-            sl.lane = *e;
-            if (k == 1 && e->lanes > 1) {
-                sl.lane.C = e->laneC[0];
-                sl.lane.est = e->laneEst[0];
-            }
-            ok = FMVD_CHECK(cudaStreamCreateWithFlags(&sl.comp, cudaStreamNonBlocking));
-            // one lane only: both slots share the work planes, so they share a stream
-            if (ok && k == 1 && e->lanes < 2) {
-                cudaStreamDestroy(sl.comp);
-                sl.comp = slot[0].comp;
-            }
             const size_t in_bytes = sizeof(S) * plane * cap_planes * V;
             const size_t out_bytes = sizeof(S) * plane * cap_planes;
-            ok = ok && FMVD_CHECK(cudaMallocHost(&sl.h_in, in_bytes)) && FMVD_CHECK(cudaMalloc(&sl.d_in, in_bytes)) &&
+            ok = FMVD_CHECK(cudaMallocHost(&sl.h_in, in_bytes)) && FMVD_CHECK(cudaMalloc(&sl.d_in, in_bytes)) &&
                  FMVD_CHECK(cudaMallocHost(&sl.h_out, out_bytes)) && FMVD_CHECK(cudaMalloc(&sl.d_out, out_bytes)) &&
                  FMVD_CHECK(cudaEventCreateWithFlags(&sl.up, cudaEventDisableTiming)) &&
                  FMVD_CHECK(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming)) &&
@@ -102,8 +104,9 @@ struct Streamer {
             if (sl.done) cudaEventDestroy(sl.done);
             if (sl.down) cudaEventDestroy(sl.down);
         }
-        if (slot[0].comp) cudaStreamDestroy(slot[0].comp);
-        if (slot[1].comp && slot[1].comp != slot[0].comp) cudaStreamDestroy(slot[1].comp);
+        for (cudaStream_t c : comp)
+            if (c)
+                cudaStreamDestroy(c);
         if (s_up) cudaStreamDestroy(s_up);
         if (s_down) cudaStreamDestroy(s_down);
     }
@@ -206,57 +209,49 @@ void deconvolve_planes(const typename Traits<S>::plan_t *plan, int iterations)
         }
     };
 
-    int cur = 0, prev = -1;
-    fill(st.slot[cur]);
-    while (true) {
-        auto &sl = st.slot[cur];
-        if (sl.n > 0) {
-            // upload: one copy per view, after the compute that last read this slot
-            if (!FMVD_CHECK(cudaStreamWaitEvent(st.s_up, sl.done, 0)))
-                return;
-            for (int v = 0; v < V; v++)
-                if (!FMVD_CHECK(cudaMemcpyAsync(sl.d_in + view_stride * v, sl.view_ptrs[v], sizeof(S) * plane * sl.n,
-                                                cudaMemcpyHostToDevice, st.s_up)))
-                    return;
-            FMVD_CHECK(cudaEventRecord(sl.up, st.s_up));
-            FMVD_CHECK(cudaStreamWaitEvent(sl.comp, sl.up, 0));
-            engine_batch(&sl.lane, sl.d_in, view_stride, sl.d_out, sl.n, iterations, sl.comp);
-            if (!FMVD_CHECK(cudaGetLastError()))
-                return;
-            FMVD_CHECK(cudaEventRecord(sl.done, sl.comp));
-            FMVD_CHECK(cudaStreamWaitEvent(st.s_down, sl.done, 0));
-            FMVD_CHECK(cudaMemcpyAsync(sl.h_out, sl.d_out, sizeof(S) * plane * sl.n, cudaMemcpyDeviceToHost,
-                                       st.s_down));
-            FMVD_CHECK(cudaEventRecord(sl.down, st.s_down));
-        }
-        // host work overlapping the device: next batch in, previous batch out
-        const int nxt = cur ^ 1;
-        auto &sn = st.slot[nxt];
-        if (prev >= 0) {
-            // slot nxt holds the previous batch: sink it before refilling
-            if (!FMVD_CHECK(cudaEventSynchronize(sn.down)))
-                return;
-            for (int i = 0; i < sn.n; i++)
-                put(sn.h_out + (size_t)i * plane);
-            sn.n = 0;
-        }
+    constexpr int K = Streamer<S>::kSlots;
+    // hands a finished batch to the datasink (planes in z order)
+    auto drain = [&](typename Streamer<S>::Slot &sl) -> bool {
+        if (sl.n == 0)
+            return true;
+        if (!FMVD_CHECK(cudaEventSynchronize(sl.down)))
+            return false;
+        for (int i = 0; i < sl.n; i++)
+            put(sl.h_out + (size_t)i * plane);
+        sl.n = 0;
+        return true;
+    };
+    int b = 0;
+    for (;; b++) {
+        auto &sl = st.slot[b % K];
+        // the slot's previous batch (b - K), the oldest in flight, goes out first
+        if (!drain(sl))
+            return;
+        fill(sl);
         if (sl.n == 0)
             break;
-        if (!FMVD_CHECK(cudaEventSynchronize(sn.up)))
-            return;
-        fill(sn);
-        prev = cur;
-        cur = nxt;
-        if (sn.n == 0) {
-            // nothing more: drain the batch just launched
-            if (!FMVD_CHECK(cudaEventSynchronize(sl.down)))
+        // upload: one copy per view (the slot's previous batch has been
+        // downloaded, so its device buffers are free)
+        for (int v = 0; v < V; v++)
+            if (!FMVD_CHECK(cudaMemcpyAsync(sl.d_in + view_stride * v, sl.view_ptrs[v], sizeof(S) * plane * sl.n,
+                                            cudaMemcpyHostToDevice, st.s_up)))
                 return;
-            for (int i = 0; i < sl.n; i++)
-                put(sl.h_out + (size_t)i * plane);
-            sl.n = 0;
-            break;
-        }
+        const int l = b % st.nlanes;
+        const cudaStream_t cs = st.comp[l];
+        if (!FMVD_CHECK(cudaEventRecord(sl.up, st.s_up)) || !FMVD_CHECK(cudaStreamWaitEvent(cs, sl.up, 0)))
+            return;
+        engine_batch(&st.lane[l], sl.d_in, view_stride, sl.d_out, sl.n, iterations, cs);
+        if (!FMVD_CHECK(cudaGetLastError()) || !FMVD_CHECK(cudaEventRecord(sl.done, cs)) ||
+            !FMVD_CHECK(cudaStreamWaitEvent(st.s_down, sl.done, 0)) ||
+            !FMVD_CHECK(cudaMemcpyAsync(sl.h_out, sl.d_out, sizeof(S) * plane * sl.n, cudaMemcpyDeviceToHost,
+                                        st.s_down)) ||
+            !FMVD_CHECK(cudaEventRecord(sl.down, st.s_down)))
+            return;
     }
+    // the batches still in flight, oldest first
+    for (int j = b - K + 1; j < b; j++)
+        if (j >= 0 && !drain(st.slot[j % K]))
+            return;
     engine_check_status(e);
 }
 

@@ -946,11 +946,14 @@ __global__ void __launch_bounds__(R * 32, 16 / R) col_pass_r(const ColArgs a)
     __syncthreads();
     column_dft(std::true_type());
     __syncthreads();
+    // row y's two elements are the 16 bytes at 16 y, column 1 first where
+    // bit 3 of y is set: one 16-byte load per row
 #pragma unroll 4
     for (int i = 0; i < H / NT; i++) {
         const int y = threadIdx.x + i * NT;
-        const float2 e0 = tile[coltile_r(y, 0)], e1 = tile[coltile_r(y, 1)];
-        *reinterpret_cast<float4 *>(C + (size_t)y * W) = make_float4(e0.x, e0.y, e1.x, e1.y);
+        const float4 e = reinterpret_cast<const float4 *>(tile)[y];
+        *reinterpret_cast<float4 *>(C + (size_t)y * W) =
+            (y >> 3) & 1 ? make_float4(e.z, e.w, e.x, e.y) : e;
     }
 }
 

@@ -20,6 +20,9 @@
 #include <stdint.h>
 #include <stdio.h>
 #include <string.h>
+#include <algorithm>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "fmvd_internal.h"
@@ -375,29 +378,87 @@ size_t source_pitch(int bits, int w)
     return ((size_t)w + a - 1) / a * a;
 }
 
+// Host copies of many bytes split over a few threads (a single thread moves
+// only a few GB/s from pageable memory).
+void host_copy(void *dst, const void *src, size_t bytes)
+{
+    constexpr size_t kPiece = size_t(4) << 20;
+    const int nt = (int)std::min<size_t>(8, bytes / kPiece);
+    if (nt < 2) {
+        memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t part = (bytes + nt - 1) / nt;
+    std::vector<std::thread> th;
+    for (int i = 1; i < nt; i++) {
+        const size_t o = part * i, n = std::min(part, bytes - o);
+        th.emplace_back([=] { memcpy((char *)dst + o, (const char *)src + o, n); });
+    }
+    memcpy(dst, src, std::min(part, bytes));
+    for (auto &t : th)
+        t.join();
+}
+
 // Upload of d source planes (host pointers, any host memory) into the
 // pitched device volume: planes are packed into two pinned staging buffers in
 // turn, each staging buffer's copy to the device running while the host
 // packs the next.
+// Pinned staging buffers of the host-memory entry points, kept for the life
+// of the process: pinning host memory costs far more than the copies through
+// it, so the buffers are allocated once and grown when a call needs more.
+// Callers hold the lock for the whole call (the reference's host-memory
+// entry points are not reentrant either).
+namespace {
+std::mutex g_stage_lock;
+void *g_stage[4] = {nullptr, nullptr, nullptr, nullptr};
+size_t g_stage_bytes[4] = {0, 0, 0, 0};
+} // namespace
+
+std::unique_lock<std::mutex> staging_lock() { return std::unique_lock<std::mutex>(g_stage_lock); }
+
+void *staging_buffer(int i, size_t bytes)
+{
+    if (g_stage_bytes[i] < bytes) {
+        cudaFreeHost(g_stage[i]);
+        g_stage[i] = nullptr;
+        g_stage_bytes[i] = 0;
+        if (!FMVD_CHECK(cudaMallocHost(&g_stage[i], bytes)))
+            return nullptr;
+        g_stage_bytes[i] = bytes;
+    }
+    return g_stage[i];
+}
+
 bool upload_planes(const void *const *h_planes, int w, int h, int d, size_t es, size_t pitch, void *d_src,
                    cudaStream_t s)
 {
     const size_t row = (size_t)w * es, plane = row * h;
-    int per = (int)(((size_t)32 << 20) / (plane ? plane : 1));
+    int per = (int)(((size_t)16 << 20) / (plane ? plane : 1));
     per = per < 1 ? 1 : (per > d ? (d > 0 ? d : 1) : per);
-    void *stage[2] = {nullptr, nullptr};
+    void *stage[2] = {staging_buffer(0, plane * per), staging_buffer(1, plane * per)};
     cudaEvent_t done[2] = {nullptr, nullptr};
-    bool ok = true;
+    bool ok = stage[0] && stage[1];
     for (int k = 0; k < 2 && ok; k++)
-        ok = FMVD_CHECK(cudaMallocHost(&stage[k], plane * per)) &&
-             FMVD_CHECK(cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming));
+        ok = FMVD_CHECK(cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming));
     bool used[2] = {false, false};
     for (int z0 = 0, k = 0; ok && z0 < d; z0 += per, k ^= 1) {
         const int n = d - z0 < per ? d - z0 : per;
         if (used[k])
             ok = FMVD_CHECK(cudaEventSynchronize(done[k]));  // the staging buffer's last copy has landed
-        for (int i = 0; ok && i < n; i++)
-            memcpy((char *)stage[k] + plane * i, h_planes[z0 + i], plane);
+        if (ok) {
+            // planes over a few threads
+            const int nt = std::max(1, std::min(8, (int)((plane * n) >> 22)));
+            std::vector<std::thread> th;
+            auto part = [&, k, z0, n, nt](int id) {
+                for (int i = id; i < n; i += nt)
+                    memcpy((char *)stage[k] + plane * i, h_planes[z0 + i], plane);
+            };
+            for (int id = 1; id < nt; id++)
+                th.emplace_back(part, id);
+            part(0);
+            for (auto &t : th)
+                t.join();
+        }
         ok = ok && FMVD_CHECK(cudaMemcpy2DAsync((char *)d_src + pitch * h * z0 * es, pitch * es, stage[k], row, row,
                                                 (size_t)h * n, cudaMemcpyHostToDevice, s)) &&
              FMVD_CHECK(cudaEventRecord(done[k], s));
@@ -407,22 +468,22 @@ bool upload_planes(const void *const *h_planes, int w, int h, int d, size_t es, 
         ok = FMVD_CHECK(cudaStreamSynchronize(s));
     else
         cudaStreamSynchronize(s);
-    for (int k = 0; k < 2; k++) {
-        cudaFreeHost(stage[k]);
+    for (int k = 0; k < 2; k++)
         if (done[k])
             cudaEventDestroy(done[k]);
-    }
     return ok;
 }
 
 // transform_cuda_* (fmvd_transform.impl.cu:77-224): upload, optional mask of
 // plane td/2, resample in chunks of planes with download and file write of
-// one chunk overlapping the resampling of the next.  Every buffer, event and
-// stream is released on every path.
+// one chunk overlapping the resampling of the next.  Every device buffer,
+// event and stream is released on every path (the pinned staging buffers are
+// the process-wide ones above).
 void transform_file(int bits, const void *const *h_planes, int w, int h, int d, int tw, int th, int td,
                     const float *h_inverse, const char *outfile, int masks, int border, float zspacing,
                     const char *maskfile)
 {
+    auto lock = staging_lock();
     const size_t es = bits == 16 ? 2 : 1;
     const size_t pitch = source_pitch(bits, w);
     void *d_src = nullptr;
@@ -462,17 +523,17 @@ void transform_file(int bits, const void *const *h_planes, int w, int h, int d, 
             for (int i = 0; i < 2 - td; i++)
                 fwrite(zero.data(), 1, plane_bytes, out);
         }
-        int chunk = (int)((256u << 20) / (plane_bytes ? plane_bytes : 1));
+        int chunk = (int)(((size_t)16 << 20) / (plane_bytes ? plane_bytes : 1));
         if (chunk < 1)
             chunk = 1;
         if (chunk > td)
             chunk = td > 0 ? td : 1;
         void *d_out[2] = {nullptr, nullptr};
-        void *h_out[2] = {nullptr, nullptr};
+        void *h_out[2] = {staging_buffer(2, plane_bytes * chunk), staging_buffer(3, plane_bytes * chunk)};
         cudaEvent_t ev[2] = {nullptr, nullptr};
+        ok = ok && h_out[0] && h_out[1];
         for (int k = 0; k < 2 && ok; k++)
             ok = FMVD_CHECK(cudaMalloc(&d_out[k], plane_bytes * chunk)) &&
-                 FMVD_CHECK(cudaMallocHost(&h_out[k], plane_bytes * chunk)) &&
                  FMVD_CHECK(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
         int pending_k = -1, pending_n = 0;
         for (int z0 = 0, k = 0; ok && z0 < td; z0 += chunk, k ^= 1) {
@@ -496,7 +557,6 @@ void transform_file(int bits, const void *const *h_planes, int w, int h, int d, 
         cudaStreamSynchronize(s);
         for (int k = 0; k < 2; k++) {
             cudaFree(d_out[k]);
-            cudaFreeHost(h_out[k]);
             if (ev[k])
                 cudaEventDestroy(ev[k]);
         }

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 
+#include <mutex>
+
 namespace fmvd {
 
 // Row pitch (samples) of the device source volume: rows padded to 16 bytes
@@ -18,6 +20,12 @@ bool resample_device(int bits, const void *d_src, size_t pitch, int w, int h, in
                      const float *h_inverse, void *d_out, float *d_outf, int *d_status, cudaStream_t s);
 void resample_direct(int bits, const void *d_src, size_t pitch, int w, int h, int d, int tw, int th, int z0, int nz,
                      const float *h_inverse, void *d_out, float *d_outf, cudaStream_t s);
+// Pinned staging buffers (index 0..3) kept for the life of the process,
+// grown on demand; hold staging_lock() while using them.
+std::unique_lock<std::mutex> staging_lock();
+void *staging_buffer(int i, size_t bytes);
+// memcpy of a large block split over a few host threads.
+void host_copy(void *dst, const void *src, size_t bytes);
 // Upload of d source planes (host pointers into any host memory, w samples
 // per row, h rows) into the pitched device volume d_src through two pinned
 // staging buffers used in turn; returns once the copies have landed.
