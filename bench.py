@@ -74,9 +74,11 @@ def parse():
     p.add_argument("--pairs-per-batch", type=int, default=0,
                    help="planes workload: plane pairs per batch (0: the library's default)")
     p.add_argument("--no-warmstart", action="store_true", help="skip the learned warm-start comparison")
-    p.add_argument("--large-train-planes", type=int, default=192,
+    p.add_argument("--large-train-planes", type=int, default=384,
                    help="large workload: frame planes whose 512 x 512 crops train the warm-start network")
-    p.add_argument("--large-epochs", type=int, default=8)
+    p.add_argument("--large-epochs", type=int, default=12)
+    p.add_argument("--large-target-iterations", type=int, default=40,
+                   help="large workload: RL iterations of the warm-start training targets")
     p.add_argument("--train-planes", type=int, default=4000)
     p.add_argument("--epochs", type=int, default=12)
     p.add_argument("--target-iterations", type=int, default=42,
@@ -430,20 +432,23 @@ def run_e2e(args, vols, mats, psfs, weights, src, frame, world=1):
     # the drop-in path as a C program drives it (C datasource and datasink):
     # resample every view into host memory, then stream the planes through
     # fmvd_initialize / deconvolve_planes / destroy_cuda_16 with nstreams 3
-    dts = []
+    frames = np.empty((V, td, th, tw), np.uint16)
     for _ in range(2):  # the first run also pages in the host buffers
         t0 = time.perf_counter()
-        frames = np.stack([api.transform_host(pinned[v], mats[v], tw, th, td) for v in range(V)])
+        for v in range(V):
+            api.transform_host(pinned[v], mats[v], tw, th, td, out=frames[v])
+        t1 = time.perf_counter()
         ref_api_out = api.deconvolve_c_callbacks(frames, weights, [p.copy() for p in psfs], 0, ITERATIONS,
                                                  nstreams=3)
-        dts.append(time.perf_counter() - t0)
+        t2 = time.perf_counter()
         assert ref_api_out.shape[0] == td
-    dt_ref_api = dts[-1]
+    dt_ref_api = t2 - t0
     return {"value": td * th * tw * ITERATIONS * world / dt, "unit": UNIT, "h2d_bytes_per_step": h2d * world,
             "d2h_bytes_per_step": d2h * world, "ms_per_step": dt * 1e3,
             "api": "fmvd_b200_reconstruct_host (pinned sources in, result to host memory)",
             "reference_style_api": {
                 "value": td * th * tw * ITERATIONS / dt_ref_api, "ms_per_step": dt_ref_api * 1e3, "gpus": 1,
+                "transform_ms": (t1 - t0) * 1e3, "deconvolve_ms": (t2 - t1) * 1e3,
                 "api": "fmvd_b200_transform_host x4 + fmvd_initialize/deconvolve_planes/destroy_cuda_16 "
                        "(frame through host memory, C datasource and datasink, nstreams 3)",
                 "h2d_bytes_per_step": h2d + V * td * th * tw * 2, "d2h_bytes_per_step": V * td * th * tw * 2 + d2h}}
@@ -626,20 +631,32 @@ def run_batched(args):
         batch.destroy()
     best = min(by_branches, key=by_branches.get)
     t_graph = by_branches[best] / 1e3
-    e0.record()
-    for p, v, o, it in zip(plans, views, outs, its):
+    # every volume on its own (CUDA events around each run), grouped by
+    # padded plane: the graph launch against the sum of the volumes' own
+    # times, and each plane class's throughput
+    per_class = {}
+    t_seq = 0.0
+    for sp, p, v, o, it in zip(specs, plans, views, outs, its):
+        e0.record()
         p.run(v, o, it)
-    e1.record()
-    torch.cuda.synchronize()
-    t_seq = e0.elapsed_time(e1) / 1e3
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        t_seq += ms / 1e3
+        c = per_class.setdefault(f"{p.fftH}x{p.fftW}", {"volumes": 0, "ms": 0.0, "padded_voxel_view_iters": 0})
+        c["volumes"] += 1
+        c["ms"] += ms
+        c["padded_voxel_view_iters"] += p.fftH * p.fftW * sp["D"] * sp["V"] * it
+    for c in per_class.values():
+        c["G_padded_voxel_view_iter_per_s"] = c["padded_voxel_view_iters"] / (c["ms"] * 1e-3) / 1e9
     for p in plans:
         p.destroy()
     print(json.dumps({
         "metric": "RL voxel-iter/s, 32 uneven volumes in one graph launch", "unit": UNIT,
         "value": voxel_iters / t_graph, "ms": t_graph * 1e3, "branches": best,
         "ms_by_branches": by_branches, "sequential_ms": t_seq * 1e3,
-        "graph_speedup": t_seq / t_graph, "volumes": len(specs), "voxel_iters": voxel_iters,
-        "dtype": "f32", "data": "synthetic",
+        "graph_speedup": t_seq / t_graph, "per_plane_class": per_class, "volumes": len(specs),
+        "voxel_iters": voxel_iters, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "batched uneven plain RL (32 volumes, planes 128..1024, depths 16..256, 2-6 views, "
                                "kernels 9..41, 25 iterations)"}}), flush=True)
 
@@ -804,13 +821,14 @@ def large_warmstart(args, plan, frame_dev):
     V, td, th, tw = frame_dev.shape
     N_RL, TOL, CROP = LARGE_ITERATIONS, 1e-2, 512
     n_train = args.large_train_planes
+    target_its = args.large_target_iterations
     z_train = 64
     z_tune, z_test = z_train + n_train + 8, z_train + n_train + 40
     t0 = time.perf_counter()
     targets = torch.empty((n_train, th, tw), dtype=torch.float32, device="cuda")
     for z0 in range(0, n_train, 16):
         n = min(16, n_train - z0)
-        est, _ = WS.rl_planes(plan, frame_dev[:, z_train + z0:z_train + z0 + n], N_RL)
+        est, _ = WS.rl_planes(plan, frame_dev[:, z_train + z0:z_train + z0 + n], target_its)
         targets[z0:z0 + n] = est
     # 512 x 512 crops on a 4 x 4 grid of every training plane
     cv, ct = [], []
@@ -855,6 +873,7 @@ def large_warmstart(args, plan, frame_dev):
             "rel_l2_vs_rl50": {"max": float(err.max()), "mean": float(err.mean()), "tolerance": TOL},
             "k_search": {str(a): b for a, b in k_errors.items()}, "network_ms_per_16_planes": t_net,
             "training": {"planes": n_train, "crops": n_crops, "crop": CROP, "epochs": args.large_epochs,
+                         "target_rl_iterations": target_its,
                          "seconds": t_train, "loss_per_epoch": hist, "data_seconds": t_data},
             "planes": {"train": [z_train, z_train + n_train], "tune": [z_tune, z_tune + 8],
                        "test": [z_test, z_test + 16]},

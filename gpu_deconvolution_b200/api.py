@@ -197,9 +197,11 @@ def deconvolve_files(view_paths, out_path, dataW, dataH, dataD, weights, kernels
 class DevicePlan:
     """Device-resident deconvolution of torch CUDA tensors (fmvd_b200.h)."""
 
-    def __init__(self, dataH, dataW, weights, kernels, psf_type=0, bits=16, pairs_per_batch=0, col_warps=0):
-        """pairs_per_batch and col_warps are the two schedule knobs (0 =
-        automatic); ``autotune.tuned_plan`` picks them by measurement."""
+    def __init__(self, dataH, dataW, weights, kernels, psf_type=0, bits=16, pairs_per_batch=0, col_warps=0,
+                 radix_step=0):
+        """pairs_per_batch, col_warps and radix_step are the schedule knobs
+        (0 = automatic; radix_step 1 or 2 selects the radix-R step of lines
+        above 1024); ``autotune.tuned_plan`` picks them by measurement."""
         self.lib = native.load()
         self.bits = bits
         self.dataH, self.dataW = dataH, dataW
@@ -209,7 +211,13 @@ class DevicePlan:
         kH, kW = self.kernels[0].shape
         native.clear_errors()
         self.plan = None
-        if col_warps:
+        if radix_step:
+            self.plan = self.lib.fmvd_b200_plan_create_scheduled(bits, dataH, dataW,
+                                                                 native.pointer_array(self.weights),
+                                                                 native.pointer_array(self.kernels), kH, kW,
+                                                                 int(psf_type), self.V, int(pairs_per_batch),
+                                                                 int(col_warps), int(radix_step))
+        elif col_warps:
             self.plan = self.lib.fmvd_b200_plan_create_tuned(bits, dataH, dataW, native.pointer_array(self.weights),
                                                              native.pointer_array(self.kernels), kH, kW,
                                                              int(psf_type), self.V, int(pairs_per_batch),
@@ -225,6 +233,7 @@ class DevicePlan:
         self.lib.fmvd_b200_plan_query(self.plan, C.byref(h), C.byref(w), C.byref(p))
         self.fftH, self.fftW, self.pairs_per_batch = h.value, w.value, p.value
         self.col_warps = self.lib.fmvd_b200_plan_col_warps(self.plan)
+        self.radix_step = self.lib.fmvd_b200_plan_radix_step(self.plan)
 
     def run(self, views, out, iterations, estimate=None, stream=0, view_stride=None, nplanes=None, init=None):
         """views: CUDA tensor holding V x D x dataH x dataW samples;
@@ -421,15 +430,18 @@ def transform_file(src: np.ndarray, inv, tw, th, td, outfile, mask=False, border
     native.check("transform_cuda")
 
 
-def transform_host(src: np.ndarray, inv, tw, th, td) -> np.ndarray:
-    """Resample into host memory (fmvd_b200_transform_host)."""
+def transform_host(src: np.ndarray, inv, tw, th, td, out: np.ndarray | None = None) -> np.ndarray:
+    """Resample into host memory (fmvd_b200_transform_host); ``out``
+    (td x th x tw, the source's sample type, contiguous) is filled if given."""
     lib = native.load()
     src = np.ascontiguousarray(src)
     bits = 16 if src.dtype == np.uint16 else 8
     d, h, w = src.shape
     planes = (C.c_void_p * d)(*[src[z].ctypes.data for z in range(d)])
     m = np.ascontiguousarray(np.asarray(inv, np.float32).reshape(12))
-    out = np.zeros((td, th, tw), src.dtype)
+    if out is None:
+        out = np.zeros((td, th, tw), src.dtype)
+    assert out.shape == (td, th, tw) and out.dtype == src.dtype and out.flags.c_contiguous
     native.clear_errors()
     r = lib.fmvd_b200_transform_host(bits, planes, w, h, d, tw, th, td, m.ctypes.data_as(native.c_float_p),
                                      out.ctypes.data)

@@ -1,13 +1,21 @@
 """Schedule autotuner for the fused RL passes.
 
-Two knobs decide how a padded plane geometry runs, and neither changes the
-arithmetic of any plane (results are bit-identical across settings):
+Three knobs decide how a padded plane geometry runs:
 
 * ``pairs_per_batch``: plane pairs deconvolved together.  Larger batches give
   each launch more blocks; smaller ones keep the batch's work planes resident
   in L2 between the four passes of a view update.
-* ``col_warps``: warps (columns) per column-pass block, 2, 4 or 8 (planes up
-  to 1024 rows), which trades shared memory per block against blocks per SM.
+* ``col_warps`` (tile schedule): warps (columns) per column-pass block, 2, 4
+  or 8 (planes up to 1024 rows), which trades shared memory per block against
+  blocks per SM.
+* ``radix_step`` (radix schedule, lines longer than 1024 = R x 512): the
+  radix-R step of the line transforms as R-point DFTs per position in shared
+  memory (1) or as each sub-line group's weighted sum over the R sub-lines
+  (2): the same transform with different instruction and shared-memory mixes.
+
+The first two never change any plane's arithmetic (results are bit-identical
+across settings); the radix schedule changes only the rounding of the FFT
+(both stay within the parity tolerance of the FP64 oracle).
 
 ``tune`` times every candidate on synthetic planes of the geometry with CUDA
 events and keeps the fastest in a JSON cache keyed by device, padded plane,
@@ -24,6 +32,7 @@ import numpy as np
 
 PAIRS = (1, 2, 3, 4, 6, 8, 12, 16)
 COL_WARPS = (2, 4, 8)
+RADIX_STEPS = (1, 2)
 MAX_WORK_BYTES = 1 << 29  # work planes of one candidate plan (C + estimate)
 
 _lock = threading.Lock()
@@ -66,9 +75,9 @@ def pair_candidates(fftH: int, fftW: int) -> list[int]:
 
 
 def best(table: dict) -> tuple:
-    """The fastest (pairs, col_warps) of a {(pairs, col_warps): ms} table;
-    ties go to the smaller batch, then the narrower block."""
-    return min(table, key=lambda k: (table[k], k[0], k[1]))
+    """The fastest (pairs, col_warps, radix_step) of a {key: ms} table; ties
+    go to the smaller batch, then the narrower block, then schedule 1."""
+    return min(table, key=lambda k: (table[k],) + tuple(k))
 
 
 def _time_candidate(plan, views, out, iterations, repeats):
@@ -87,7 +96,8 @@ def _time_candidate(plan, views, out, iterations, repeats):
 def tune(dataH, dataW, kH, kW, views=4, bits=16, planes=48, iterations=2, repeats=2, use_cache=True,
          path=None) -> dict:
     """Measure (or read from the cache) the best schedule for a geometry.
-    Returns {"pairs_per_batch", "col_warps", "ms", "fft", "table"}."""
+    Returns {"pairs_per_batch", "col_warps", "radix_step", "ms", "fft",
+    "table"}."""
     import torch
 
     from . import api, native, synth
@@ -112,22 +122,24 @@ def tune(dataH, dataW, kH, kW, views=4, bits=16, planes=48, iterations=2, repeat
     psfs = [synth.gaussian_psf(kH, kW, 1.2, 3.0, 40.0 * v) for v in range(views)]
     weights = [np.ones((dataH, dataW), np.float32)] * views
     cws = COL_WARPS if fftH <= 1024 else (0,)
+    radix = RADIX_STEPS if max(fftH, fftW) > 1024 else (1,)
     table = {}
     for pairs in pair_candidates(fftH, fftW):
         for cw in cws:
-            try:
-                plan = api.DevicePlan(dataH, dataW, weights, [p.copy() for p in psfs], 0, bits=bits,
-                                      pairs_per_batch=pairs, col_warps=cw)
-            except native.FmvdError:
-                continue  # this column width does not fit the plane
-            try:
-                table[(pairs, plan.col_warps)] = _time_candidate(plan, vols, out, iterations, repeats)
-            finally:
-                plan.destroy()
-    pairs, cw = best(table)
-    entry = {"pairs_per_batch": pairs, "col_warps": cw, "ms": table[(pairs, cw)], "fft": [fftH, fftW],
-             "planes": planes, "iterations": iterations,
-             "table": {f"{p},{c}": round(ms, 4) for (p, c), ms in sorted(table.items())}}
+            for rs in radix:
+                try:
+                    plan = api.DevicePlan(dataH, dataW, weights, [p.copy() for p in psfs], 0, bits=bits,
+                                          pairs_per_batch=pairs, col_warps=cw, radix_step=rs)
+                except native.FmvdError:
+                    continue  # this column width does not fit the plane
+                try:
+                    table[(pairs, plan.col_warps, rs)] = _time_candidate(plan, vols, out, iterations, repeats)
+                finally:
+                    plan.destroy()
+    pairs, cw, rs = best(table)
+    entry = {"pairs_per_batch": pairs, "col_warps": cw, "radix_step": rs, "ms": table[(pairs, cw, rs)],
+             "fft": [fftH, fftW], "planes": planes, "iterations": iterations,
+             "table": {f"{p},{c},{r}": round(ms, 4) for (p, c, r), ms in sorted(table.items())}}
     if use_cache:
         save_entry(key, entry, path)
     return entry
@@ -139,4 +151,5 @@ def tuned_plan(dataH, dataW, weights, kernels, psf_type=0, bits=16, **tune_args)
     kH, kW = np.asarray(kernels[0]).shape
     t = tune(dataH, dataW, kH, kW, views=len(kernels), bits=bits, **tune_args)
     return api.DevicePlan(dataH, dataW, weights, kernels, psf_type, bits=bits,
-                          pairs_per_batch=t["pairs_per_batch"], col_warps=t["col_warps"])
+                          pairs_per_batch=t["pairs_per_batch"], col_warps=t["col_warps"],
+                          radix_step=t.get("radix_step", 0))

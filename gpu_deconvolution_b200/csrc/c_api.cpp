@@ -107,6 +107,28 @@ fmvd_b200_plan *fmvd_b200_plan_create_tuned(int bits, int dataH, int dataW, cons
     return new fmvd_b200_plan{e};
 }
 
+fmvd_b200_plan *fmvd_b200_plan_create_scheduled(int bits, int dataH, int dataW, const float *const *h_Weights,
+                                                float **h_Kernel, int kernelH, int kernelW,
+                                                fmvd_psf_type iteration_type, int nViews, int pairs_per_batch,
+                                                int col_warps, int radix_step)
+{
+    if (radix_step < 0 || radix_step > 2) {
+        fmvd::report_error("fmvd: radix_step must be 0, 1 or 2");
+        return nullptr;
+    }
+    fmvd::Engine *e = fmvd::engine_create(bits, dataH, dataW, h_Weights, h_Kernel, kernelH, kernelW, iteration_type,
+                                          nViews, pairs_per_batch, col_warps);
+    if (!e)
+        return nullptr;
+    e->dims.radix_step = radix_step == 2 ? fmvd::kRadixSums : fmvd::kRadixDft;
+    return new fmvd_b200_plan{e};
+}
+
+int fmvd_b200_plan_radix_step(const fmvd_b200_plan *plan)
+{
+    return plan ? (plan->eng->dims.radix_step == fmvd::kRadixSums ? 2 : 1) : -1;
+}
+
 int fmvd_b200_plan_col_warps(const fmvd_b200_plan *plan) { return plan ? plan->eng->dims.col_warps : -1; }
 
 int fmvd_b200_plan_query(const fmvd_b200_plan *plan, int *fftH, int *fftW, int *pairs)

@@ -216,6 +216,7 @@ Engine *engine_create(int bits, int dataH, int dataW, const float *const *h_Weig
     e->dims.byW = kH / 2;
     e->dims.bxW = kW / 2;
     e->dims.col_warps = cw;
+    e->dims.radix_step = kRadixDft;
     e->kH = kH;
     e->kW = kW;
     e->device = dev;

@@ -688,11 +688,21 @@ __device__ __forceinline__ void line_twiddle(float2 *v, const float2 *__restrict
     }
 }
 
+// w_R^(r j) (twN: w_N^n with N = R * kLineM)
+template <int R>
+__device__ __forceinline__ float2 line_coefficient(const float2 *__restrict__ twN, int r, int j)
+{
+    return __ldg(twN + ((r * j) % R) * kLineM);
+}
+
 // Row pass for W = R * 512: R warps, two rows per block (half-warp h of warp
 // r is group r of row h).
 // SMEM: the launch bulk-copies each row's weight row (update) or data rows
 // (divide) into shared memory after the buffers.
-template <int R, int MODE, int BITS, bool NOOUT, bool SMEM>
+// DSTEP: the radix-R step as R-point DFTs per position (true) or as each
+// group's weighted sum over all R sub-lines (false); the two schedules give
+// the same transform with different instruction mixes (autotuner knob).
+template <int R, int MODE, int BITS, bool NOOUT, bool SMEM, bool DSTEP>
 __global__ void __launch_bounds__(R * 32, 16 / R) row_pass_r(const RowArgs a)
 {
     using WF = WarpFft<kLineM>;
@@ -740,6 +750,21 @@ __global__ void __launch_bounds__(R * 32, 16 / R) row_pass_r(const RowArgs a)
         for (int m = 0; m < E; m++)
             buf[t + T * m] = v[m];
         __syncthreads();
+        if constexpr (!DSTEP) {
+            // each group sums all R sub-lines at its own positions
+#pragma unroll
+            for (int m = 0; m < E; m++)
+                v[m] = lbuf[t + T * m];
+#pragma unroll
+            for (int j = 1; j < R; j++) {
+                const float2 cj = line_coefficient<R>(a.twN, r, j);
+#pragma unroll
+                for (int m = 0; m < E; m++)
+                    v[m] = cadd(v[m], cmul(lbuf[j * PF2 + t + T * m], cj));
+            }
+            __syncthreads();
+            return;
+        }
 #pragma unroll 1
         for (int b = r; b < kLineM / 16; b += R) {
             float2 z[R];
@@ -860,7 +885,7 @@ __device__ __forceinline__ void col_fft_512(float2 *v, const TW &tw, uint32_t wb
 // Column pass for H = R * 512: R warps, two columns per block (half-warp cc
 // of warp r is group r of column cc).  Spectrum in launch layout: block bx,
 // register m, thread tid at spec[(bx * 32 + m) * (32 R) + tid].
-template <int R>
+template <int R, bool DSTEP>
 __global__ void __launch_bounds__(R * 32, 16 / R) col_pass_r(const ColArgs a)
 {
     using WF = WarpFft<kLineM>;
@@ -908,6 +933,25 @@ __global__ void __launch_bounds__(R * 32, 16 / R) col_pass_r(const ColArgs a)
         }
     };
 
+    // the other schedule: v[m] = sum_j (row 512 j + t + 16 m of this column) w_R^(r j)
+    const auto column_sum = [&](float2 *v) {
+#pragma unroll
+        for (int m = 0; m < E; m++)
+            v[m] = lds2(col + 256u * m);
+#pragma unroll
+        for (int j = 1; j < R; j++) {
+            const float2 cj = line_coefficient<R>(a.twN, r, j);
+#pragma unroll
+            for (int m0 = 0; m0 < E; m0 += 8) {
+                asm volatile("" ::: "memory");  // bounds the loads in flight
+#pragma unroll
+                for (int m = m0; m < m0 + 8; m++)
+                    v[m] = cadd(v[m], cmul(lds2(col + 8192u * j + 256u * m), cj));
+            }
+        }
+        asm volatile("" ::: "memory");
+    };
+
     float2 v[E];
     // pass 0: space -> frequency, times the spectrum, conjugated; pass 1:
     // the same forward pipeline then runs frequency -> space.  The rolled
@@ -917,12 +961,17 @@ __global__ void __launch_bounds__(R * 32, 16 / R) col_pass_r(const ColArgs a)
 #pragma unroll 1
     for (int pass = 0; pass < 2; pass++) {
         if (pass == 0) {
-            column_dft(std::false_type());
-            __syncthreads();  // every block of positions has its radix-R step
+            if constexpr (DSTEP) {
+                column_dft(std::false_type());
+                __syncthreads();  // every block of positions has its radix-R step
 #pragma unroll
-            for (int m = 0; m < E; m++)
-                v[m] = lds2(col + 8192u * r + 256u * m);  // row 512 r + t + 16 m: this group's sub-line
-            __syncwarp();  // read before this warp's transposes overwrite its segment
+                for (int m = 0; m < E; m++)
+                    v[m] = lds2(col + 8192u * r + 256u * m);  // row 512 r + t + 16 m: this group's sub-line
+                __syncwarp();  // read before this warp's transposes overwrite its segment
+            } else {
+                column_sum(v);
+                __syncthreads();  // every group has read the column before transposes overwrite it
+            }
             line_twiddle(v, a.twN, r, t);
         }
         col_fft_512<-1>(v, a.tw, wbase, rbase, t);
@@ -944,7 +993,15 @@ __global__ void __launch_bounds__(R * 32, 16 / R) col_pass_r(const ColArgs a)
     for (int m = 0; m < E; m++)
         sts2(seg + q + 256u * m, v[m]);  // row 512 r + t + 16 m
     __syncthreads();
-    column_dft(std::true_type());
+    if constexpr (DSTEP) {
+        column_dft(std::true_type());
+    } else {
+        column_sum(v);
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < E; m++)
+            sts2(seg + q + 256u * m, make_float2(v[m].x, -v[m].y));
+    }
     __syncthreads();
     // row y's two elements are the 16 bytes at 16 y, column 1 first where
     // bit 3 of y is set: one 16-byte load per row
@@ -1196,31 +1253,31 @@ static void pick_row_w(bool noout, bool sm, void (*&kern)(const RowArgs), unsign
 
 // Line-engine row-pass variant for a launch (per sample width; update
 // passes per last / not last).
-template <int R, int MODE, int BITS>
+template <int R, int MODE, int BITS, bool DSTEP>
 static void pick_row_r_bits(bool noout, bool sm, void (*&kern)(const RowArgs), unsigned *&m)
 {
     static unsigned mask[4] = {0, 0, 0, 0};
     constexpr bool U = MODE == ROW_UPDATE;
     if (noout)
-        kern = sm ? row_pass_r<R, MODE, BITS, U, true> : row_pass_r<R, MODE, BITS, U, false>;
+        kern = sm ? row_pass_r<R, MODE, BITS, U, true, DSTEP> : row_pass_r<R, MODE, BITS, U, false, DSTEP>;
     else
-        kern = sm ? row_pass_r<R, MODE, BITS, false, true> : row_pass_r<R, MODE, BITS, false, false>;
+        kern = sm ? row_pass_r<R, MODE, BITS, false, true, DSTEP> : row_pass_r<R, MODE, BITS, false, false, DSTEP>;
     m = &mask[(noout ? 1 : 0) + (sm ? 2 : 0)];
 }
 
 // (sm: the operand rows may be bulk-copied into shared memory)
-template <int R, int MODE>
+template <int R, int MODE, bool DSTEP>
 static void pick_row_r(const RowArgs &a, bool sm, void (*&kern)(const RowArgs), unsigned *&m)
 {
     static unsigned mask0 = 0;
     const bool noout = MODE == ROW_UPDATE && !a.last;
     if constexpr (MODE == ROW_INIT) {
-        kern = row_pass_r<R, MODE, 0, false, false>;
+        kern = row_pass_r<R, MODE, 0, false, false, DSTEP>;
         m = &mask0;
     } else if (a.d.bits == 16) {
-        pick_row_r_bits<R, MODE, 16>(noout, sm, kern, m);
+        pick_row_r_bits<R, MODE, 16, DSTEP>(noout, sm, kern, m);
     } else {
-        pick_row_r_bits<R, MODE, 8>(noout, sm, kern, m);
+        pick_row_r_bits<R, MODE, 8, DSTEP>(noout, sm, kern, m);
     }
 }
 
@@ -1280,7 +1337,10 @@ static void launch_row(const RowArgs &a0, cudaStream_t s)
         }
         void (*kern)(const RowArgs);
         unsigned *m;
-        pick_row_r<R, MODE>(a, sm, kern, m);
+        if (a.d.radix_step == kRadixSums)
+            pick_row_r<R, MODE, false>(a, sm, kern, m);
+        else
+            pick_row_r<R, MODE, true>(a, sm, kern, m);
         configure_smem(kern, 200 * 1024, *m);
         dim3 grid(a.d.H / 2, a.b.npairs);
         kern<<<grid, R * 32, smem, s>>>(a);
@@ -1303,7 +1363,7 @@ static void launch_col_w(const ColArgs &a, int npairs, cudaStream_t s)
 }
 
 template <int H>
-static void launch_col(const ColArgs &a, int npairs, int cw, cudaStream_t s)
+static void launch_col(const ColArgs &a, int npairs, int cw, int radix_step, cudaStream_t s)
 {
     if constexpr (H <= 1024) {
         switch (cw) {
@@ -1315,9 +1375,10 @@ static void launch_col(const ColArgs &a, int npairs, int cw, cudaStream_t s)
         constexpr int R = H / kLineM;
         static_assert(H % kLineM == 0 && R >= 3 && R <= 8, "columns above 1024 are 3..8 sub-lines of 512");
         constexpr size_t smem = sizeof(float2) * 2 * H + 256;  // tile aligned to 256 bytes in the kernel
-        auto kern = col_pass_r<R>;
-        static unsigned mask = 0;
-        configure_smem(kern, smem, mask);
+        const bool sums = radix_step == kRadixSums;
+        auto kern = sums ? col_pass_r<R, false> : col_pass_r<R, true>;
+        static unsigned mask[2] = {0, 0};
+        configure_smem(kern, smem, mask[sums ? 1 : 0]);
         dim3 grid(a.W / 2, npairs);
         kern<<<grid, R * 32, smem, s>>>(a);
     }
@@ -1359,7 +1420,7 @@ void rl_col(const RlDims &d, const RlBatch &b, const RlTables &t, const float2 *
     ColArgs a{b.C, spectrum, t.wtwH, d.H, d.W, t.twH};
     switch (d.H) {
 #define X(N) \
-    case N: launch_col<N>(a, b.npairs, d.col_warps ? d.col_warps : col_warps(d.H, d.W), s); break;
+    case N: launch_col<N>(a, b.npairs, d.col_warps ? d.col_warps : col_warps(d.H, d.W), d.radix_step, s); break;
         FMVD_FOR_EACH_LENGTH(X)
 #undef X
     default: break;

@@ -18,7 +18,14 @@ struct RlDims {
     int byD, bxD;
     int byW, bxW;
     int col_warps;       // column-pass warps per block (warp engine, H <= 1024)
+    int radix_step;      // lines above 1024: kRadixDft or kRadixSums
 };
+
+// Schedules of the radix-R step of lines above 1024 (same transform): R-point
+// DFTs per position in shared memory, or each group's weighted sum over the
+// R sub-lines.
+constexpr int kRadixDft = 1;
+constexpr int kRadixSums = 2;
 
 // One batch of plane pairs resident on the device.  Pair p packs planes
 // 2p (real part) and 2p+1 (imaginary part).

@@ -112,6 +112,9 @@ SIGNATURES = {
     "fmvd_b200_batch_destroy": (None, [c_p]),
     "fmvd_b200_plan_create_tuned": (c_p, [c_int, c_int, c_int, c_p, c_p, c_int, c_int, c_int, c_int, c_int, c_int]),
     "fmvd_b200_plan_col_warps": (c_int, [c_p]),
+    "fmvd_b200_plan_create_scheduled": (c_p, [c_int, c_int, c_int, c_p, c_p, c_int, c_int, c_int, c_int, c_int,
+                                             c_int, c_int]),
+    "fmvd_b200_plan_radix_step": (c_int, [c_p]),
     "fmvd_b200_deconvolve_device_from": (c_int, [c_p, c_p, C.c_size_t, c_p, c_int, c_int, c_p, c_p, c_p]),
     "fmvd_b200_pad_estimate": (c_int, [c_p, c_p, c_p, c_int, C.c_float, c_p]),
     "fmvd_b200_plane_stats": (c_int, [c_p, c_p, c_int, c_int, c_int, c_int, c_int, c_p, c_p]),

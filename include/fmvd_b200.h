@@ -31,6 +31,17 @@ int fmvd_b200_plan_query(const fmvd_b200_plan *plan, int *fftH, int *fftW, int *
 fmvd_b200_plan *fmvd_b200_plan_create_tuned(int bits, int dataH, int dataW, const float *const *h_Weights,
                                             float **h_Kernel, int kernelH, int kernelW, fmvd_psf_type iteration_type,
                                             int nViews, int pairs_per_batch, int col_warps);
+/* fmvd_b200_plan_create_tuned with the radix schedule of lines longer than
+ * 1024 as well: radix_step = 1 runs the radix-R step of the R x 512 line
+ * transforms as R-point DFTs per position, 2 as each sub-line group's
+ * weighted sum over the R sub-lines (the same transform with a different
+ * instruction mix), 0 the default (1).  The autotuner's third knob. */
+fmvd_b200_plan *fmvd_b200_plan_create_scheduled(int bits, int dataH, int dataW, const float *const *h_Weights,
+                                                float **h_Kernel, int kernelH, int kernelW,
+                                                fmvd_psf_type iteration_type, int nViews, int pairs_per_batch,
+                                                int col_warps, int radix_step);
+/* The plan's radix schedule (1 or 2, as above). */
+int fmvd_b200_plan_radix_step(const fmvd_b200_plan *plan);
 /* Column-pass warps per block of the plan (0 for planes above 1024 rows,
  * whose column pass has a fixed two-column tile). */
 int fmvd_b200_plan_col_warps(const fmvd_b200_plan *plan);

@@ -13,6 +13,8 @@ def test_best_prefers_fastest_then_smaller():
     table = {(2, 4): 1.0, (4, 8): 0.8, (6, 2): 0.8, (1, 2): 3.0}
     assert autotune.best(table) == (4, 8)
     assert autotune.best({(3, 8): 1.0, (3, 4): 1.0}) == (3, 4)
+    # with the radix schedule as the third knob
+    assert autotune.best({(1, 0, 2): 0.5, (1, 0, 1): 0.6, (2, 0, 1): 0.5}) == (1, 0, 2)
 
 
 def test_pair_candidates_bounded_by_memory():
@@ -155,19 +157,24 @@ def test_tuned_plan_is_bit_identical(tmp_path):
         default.destroy()
 
 
+def _oracle_middle_plane(args):
+    H, W, weights, psfs, planes, iterations = args
+    from oracle import fmvd_oracle as Or
+    return Or.Plan(H, W, weights, psfs, 0).deconvolve_plane(planes, iterations)
+
+
 @pytest.mark.gpu
 def test_batched_workload_volumes_against_oracle():
     """Per-volume error of the batched workload (32 volumes, seed 0) against
-    the FP64 oracle, on the middle plane of every volume whose padded plane is
-    at most 512 x 512 (the oracle's cost bounds the rest): within the RL
-    parity tolerance of 1e-4 relative L2."""
+    the FP64 oracle, on the middle plane of every volume (padded planes 256
+    to 1536), within the RL parity tolerance of 1e-4 relative L2.  The
+    oracle's planes run in spawned processes."""
+    import multiprocessing as mp
+
     import torch
     from gpu_deconvolution_b200 import api
-    from oracle import fmvd_oracle as O
-    checked = 0
+    jobs, ests, idx = [], [], []
     for sp in synth.batched_specs(0, 32):
-        if O.snap_transform_size(sp["H"] + sp["k"] - 1) > 512:
-            continue
         psfs = synth.spec_psfs(sp)
         w = [np.ones((sp["H"], sp["W"]), np.float32)] * sp["V"]
         views = synth.views_torch(sp)
@@ -182,8 +189,51 @@ def test_batched_workload_volumes_against_oracle():
         finally:
             plan.destroy()
         vv = one[:, 0].cpu().numpy().view(np.uint16)
-        ref = O.Plan(sp["H"], sp["W"], w, psfs, 0).deconvolve_plane([vv[v] for v in range(sp["V"])],
-                                                                    sp["iterations"])
-        assert rel_l2(est[0].cpu().numpy(), ref) < 1e-4, sp["index"]
-        checked += 1
-    assert checked >= 5
+        jobs.append((sp["H"], sp["W"], w, psfs, [vv[v] for v in range(sp["V"])], sp["iterations"]))
+        ests.append(est[0].cpu().numpy())
+        idx.append(sp["index"])
+        del views
+    with mp.get_context("spawn").Pool(min(16, len(jobs))) as pool:
+        refs = pool.map(_oracle_middle_plane, jobs)
+    errors = {i: rel_l2(e, r) for i, e, r in zip(idx, ests, refs)}
+    print("per-volume rel L2 vs the FP64 oracle:", {i: f"{v:.2e}" for i, v in errors.items()})
+    assert len(errors) == 32
+    assert max(errors.values()) < 1e-4, errors
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fh,fw", [(1536, 64), (64, 2560), (3072, 64)])
+def test_radix_schedules_match_oracle(fh, fw):
+    """Both radix schedules of lines above 1024 (R-point DFTs per position,
+    and weighted sums over the sub-lines) against the FP64 oracle, in the row
+    and the column role."""
+    import torch
+    from gpu_deconvolution_b200 import api
+    from oracle import fmvd_oracle as O
+    k = 7
+    H, W = fh - k + 1, fw - k + 1
+    rng = np.random.default_rng(fh + fw)
+    views = rng.integers(20, 3000, (2, 3, H, W)).astype(np.uint16)
+    psfs = [synth.gaussian_psf(k, k, 1.0, 2.0, 40.0 * v) for v in range(2)]
+    w = [rng.uniform(0.3, 1.5, (H, W)).astype(np.float32) for _ in range(2)]
+    _, oest = O.deconvolve_volume(views, w, psfs, 0, 3, return_float=True)
+    tv = torch.from_numpy(views.view(np.int16)).cuda()
+    for rs in (1, 2):
+        plan = api.DevicePlan(H, W, w, [p.copy() for p in psfs], 0, radix_step=rs)
+        try:
+            assert plan.radix_step == rs
+            out = torch.zeros((3, H, W), dtype=torch.int16, device="cuda")
+            est = torch.zeros((3, plan.fftH, plan.fftW), dtype=torch.float32, device="cuda")
+            plan.run(tv, out, 3, estimate=est)
+            torch.cuda.synchronize()
+            assert rel_l2(est.cpu().numpy(), oest) < 1e-4, rs
+        finally:
+            plan.destroy()
+
+
+@pytest.mark.gpu
+def test_tuner_picks_radix_schedule(tmp_path):
+    entry = autotune.tune(1400, 1400, 31, 31, views=2, planes=4, iterations=1, repeats=1,
+                          path=str(tmp_path / "t.json"))
+    assert entry["radix_step"] in (1, 2) and entry["fft"] == [1536, 1536]
+    assert any(key.endswith(",2") for key in entry["table"]) and any(key.endswith(",1") for key in entry["table"])
