@@ -811,10 +811,12 @@ def large_warmstart(args, plan, frame_dev):
     2048 x 2048 planes (6 views, 63 x 63 PSFs, transformed-mask weights).
 
     The network (6 views + their mean in, BF16 tcgen05 kernels) is trained on
-    512 x 512 crops of registered frame planes with targets = the same crops
-    of the planes' plain RL-50 results; it then runs on whole 2048 x 2048
-    planes (the same parameters in a network sized for them).  k is tuned on
-    held-out planes, and both paths are timed on test planes; training,
+    the 512 x 512 tiles of registered frame planes (a 4 x 4 grid) with targets
+    = the same tiles of the planes' plain RL results (--large-target-iterations
+    iterations, fewer than 50 so that a few RL iterations after the warm
+    start reach the RL-50 result); at inference it runs on the same tiling of
+    whole planes, and RL-k continues from the stitched estimate.  k is tuned
+    on held-out planes, and both paths are timed on test planes; training,
     tuning and test planes are disjoint plane ranges of the frame."""
     import torch
     from gpu_deconvolution_b200 import warmstart as WS
@@ -850,24 +852,43 @@ def large_warmstart(args, plan, frame_dev):
     n_crops = crop_views.shape[1]
     del crop_views, crop_targets
     torch.cuda.empty_cache()
-    full = WS.WarmStartNet(th, tw, V, max_batch=2, seed=0)
-    full.set_params(net.params())
-    net.destroy()
+    # inference on the same 512 x 512 tiling as the training crops (the
+    # network normalises its input per tile, so tiles must match training)
+    ny, nx = th // CROP, tw // CROP
+
+    def tiled_guess(views):
+        Vv, N = views.shape[:2]
+        tiles = views.reshape(Vv, N, ny, CROP, nx, CROP).permute(0, 1, 2, 4, 3, 5).reshape(Vv, N * ny * nx, CROP, CROP)
+        g = net.forward(tiles.contiguous())
+        return g.reshape(N, ny, nx, CROP, CROP).permute(0, 1, 3, 2, 4).reshape(N, th, tw).contiguous()
+
+    def warm(views, k):
+        guess = tiled_guess(views)
+        init = torch.empty((views.shape[1], plan.fftH, plan.fftW), dtype=torch.float32, device="cuda")
+        plan.pad_estimate(guess, init, 1.0)
+        est, _ = WS.rl_planes(plan, views, k, init=init)
+        return est
+
     tune_views = frame_dev[:, z_tune:z_tune + 8].contiguous()
     test_views = frame_dev[:, z_test:z_test + 16].contiguous()
     tune_ref, _ = WS.rl_planes(plan, tune_views, N_RL)
     tune_ref = tune_ref.contiguous()
-    k, k_errors = WS.tune_k(full, plan, tune_views, tune_ref, TOL,
-                            candidates=tuple(range(0, 13)) + (14, 16, 20, 25, 30, 40))
+    k, k_errors = None, {}
+    for cand in tuple(range(0, 13)) + (14, 16, 20, 25, 30, 40):
+        err = float(np.max(WS.rel_l2_planes(warm(tune_views, cand).contiguous(), tune_ref)))
+        k_errors[cand] = err
+        if err <= TOL:
+            k = cand
+            break
     kk = k if k is not None else N_RL
     t_plain = WS.time_cuda(lambda: WS.rl_planes(plan, test_views, N_RL))
-    t_warm = WS.time_cuda(lambda: WS.warm_deconvolve(full, plan, test_views, kk))
-    t_net = WS.time_cuda(lambda: full.forward(test_views))
-    warm, _ = WS.warm_deconvolve(full, plan, test_views, kk)
+    t_warm = WS.time_cuda(lambda: warm(test_views, kk))
+    t_net = WS.time_cuda(lambda: tiled_guess(test_views))
+    warm_est = warm(test_views, kk)
     plain, _ = WS.rl_planes(plan, test_views, N_RL)
-    err = WS.rel_l2_planes(warm.contiguous(), plain.contiguous())
-    full.check()
-    full.destroy()
+    err = WS.rel_l2_planes(warm_est.contiguous(), plain.contiguous())
+    net.check()
+    net.destroy()
     return {"metric": "time to the plain RL-50 result, warm start vs plain", "unit": "ms per 16 planes",
             "value": t_warm, "plain_rl50_ms": t_plain, "speedup": t_plain / t_warm, "k": k,
             "rel_l2_vs_rl50": {"max": float(err.max()), "mean": float(err.mean()), "tolerance": TOL},

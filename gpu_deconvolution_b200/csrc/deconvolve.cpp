@@ -38,6 +38,16 @@ struct Traits<unsigned char> {
     static constexpr int bits = 8;
 };
 
+// FMVD_STRICT_READ_AHEAD=1 in the environment: streaming plans read ahead
+// no further than the reference (nstreams planes before the first datasink
+// call), for datasources that cannot deliver a plane before earlier ones were
+// returned; one batch of at most nstreams planes is in flight at a time.
+bool strict_read_ahead()
+{
+    const char *v = getenv("FMVD_STRICT_READ_AHEAD");
+    return v && v[0] && v[0] != '0';
+}
+
 template <typename S>
 struct Streamer {
     // Three batch slots over the engine's two lanes: batch b fills slot
@@ -46,6 +56,7 @@ struct Streamer {
     static constexpr int kSlots = 3;
     Engine *eng = nullptr;
     int cap_planes = 0;
+    int nslots = kSlots;  // 1 in the strict read-ahead mode
     size_t plane = 0;
     struct Slot {
         S *h_in = nullptr, *d_in = nullptr, *h_out = nullptr, *d_out = nullptr;
@@ -58,10 +69,16 @@ struct Streamer {
     int nlanes = 1;
     cudaStream_t s_up = nullptr, s_down = nullptr;
 
-    bool init(Engine *e)
+    bool init(Engine *e, int nstreams)
     {
         eng = e;
         cap_planes = 2 * e->pairs_cap;
+        if (strict_read_ahead()) {
+            // the datasource runs at most nstreams planes (and at most one
+            // batch) ahead of the datasink, as in the reference
+            nslots = 1;
+            cap_planes = nstreams < cap_planes ? nstreams : cap_planes;
+        }
         plane = (size_t)e->dims.dataH * e->dims.dataW;
         const int V = e->dims.V;
         nlanes = e->lanes > 1 ? 2 : 1;
@@ -74,7 +91,7 @@ struct Streamer {
                   FMVD_CHECK(cudaStreamCreateWithFlags(&s_down, cudaStreamNonBlocking));
         for (int l = 0; l < nlanes && ok; l++)
             ok = FMVD_CHECK(cudaStreamCreateWithFlags(&comp[l], cudaStreamNonBlocking));
-        for (int k = 0; k < kSlots && ok; k++) {
+        for (int k = 0; k < nslots && ok; k++) {
             Slot &sl = slot[k];
             const size_t in_bytes = sizeof(S) * plane * cap_planes * V;
             const size_t out_bytes = sizeof(S) * plane * cap_planes;
@@ -133,7 +150,7 @@ typename Traits<S>::plan_t *initialize(int dataH, int dataW, const float *const 
     if (!e)
         return nullptr;
     Plan<S> *p = new Plan<S>();
-    if (!p->st.init(e)) {
+    if (!p->st.init(e, nstreams)) {
         p->st.release();
         engine_destroy(e);
         delete p;
@@ -209,7 +226,7 @@ void deconvolve_planes(const typename Traits<S>::plan_t *plan, int iterations)
         }
     };
 
-    constexpr int K = Streamer<S>::kSlots;
+    const int K = st.nslots;
     // hands a finished batch to the datasink (planes in z order)
     auto drain = [&](typename Streamer<S>::Slot &sl) -> bool {
         if (sl.n == 0)

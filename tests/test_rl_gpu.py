@@ -174,6 +174,33 @@ def test_streaming_c_callbacks_match_device_api():
     assert stats["source_calls"] == 14 and stats["sink_calls"] == 13
 
 
+def test_streaming_strict_read_ahead(monkeypatch):
+    """FMVD_STRICT_READ_AHEAD=1: the datasource never runs more than nstreams
+    planes ahead of the datasink (the reference's read-ahead), and the planes
+    are the same as with batched read-ahead."""
+    views, psfs, weights, _ = synth.plain_rl_views(shape=(9, 40, 44), n_views=2, n_beads=10, ksize=9, seed=17)
+    want = api.deconvolve(views, weights, [p.copy() for p in psfs], 0, 2, nstreams=3)
+    monkeypatch.setenv("FMVD_STRICT_READ_AHEAD", "1")
+    state = {"z": 0, "out": [], "ahead": 0}
+
+    def source(bufs):
+        if state["z"] >= views.shape[1]:
+            return False
+        for v in range(views.shape[0]):
+            bufs[v][...] = views[v, state["z"]]
+        state["z"] += 1
+        state["ahead"] = max(state["ahead"], state["z"] - len(state["out"]))
+        return True
+
+    plan = api.StreamingPlan(40, 44, weights, [p.copy() for p in psfs], 0, 3, source, state["out"].append)
+    try:
+        plan.deconvolve_planes(2)
+    finally:
+        plan.destroy()
+    assert np.array_equal(np.stack(state["out"]), want)
+    assert state["ahead"] <= 3
+
+
 def test_streaming_fewer_planes_than_streams():
     """Reference quirk: a source with 1 plane and nstreams = 3 gives 3 sink
     calls and 4 source calls; the first plane is the real result."""
