@@ -780,9 +780,27 @@ def run_large(args):
             dt = time.perf_counter() - t0
         finally:
             rec.destroy()
+        # the same transfers alone (pinned host memory, one copy per view up,
+        # the result down): how much of them the pipelined run hides
+        dev_buf = torch.empty((d, h, w), dtype=torch.int16, device="cuda")
+        res_host = torch.empty((td, th, tw), dtype=torch.int16, pin_memory=True)
+        res_dev = torch.empty((td, th, tw), dtype=torch.int16, device="cuda")
+        c0, c1, c2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        c0.record()
+        for v in range(V):
+            dev_buf.copy_(pinned[v], non_blocking=True)
+        c1.record()
+        res_host.copy_(res_dev, non_blocking=True)
+        c2.record()
+        torch.cuda.synchronize()
+        t_h2d, t_d2h = c0.elapsed_time(c1) / 1e3, c1.elapsed_time(c2) / 1e3
+        del dev_buf, res_dev, res_host
+        t_dev = t_total / args.steps
         e2e = {"value": voxel_iters / dt, "unit": UNIT, "ms_per_step": dt * 1e3,
                "h2d_bytes_per_step": V * d * h * w * 2, "d2h_bytes_per_step": td * th * tw * 2,
-               "api": "fmvd_b200_reconstruct_host (pinned sources in, result to host memory)"}
+               "api": "fmvd_b200_reconstruct_host (pinned sources in, result to host memory)",
+               "copies_alone_ms": {"h2d": t_h2d * 1e3, "d2h": t_d2h * 1e3},
+               "hidden_fraction_of_copies": max(0.0, min(1.0, (t_dev + t_h2d + t_d2h - dt) / (t_h2d + t_d2h)))}
     cpu = cpu_baseline(frames_cpu, weights, psfs, iterations=1) if frames_cpu is not None else None
     plan.destroy()
     print(json.dumps({

@@ -763,23 +763,23 @@ __global__ void __launch_bounds__(R * 32, 16 / R) row_pass_r(const RowArgs a)
                     v[m] = cadd(v[m], cmul(lbuf[j * PF2 + t + T * m], cj));
             }
             __syncthreads();
-            return;
-        }
+        } else {
 #pragma unroll 1
-        for (int b = r; b < kLineM / 16; b += R) {
-            float2 z[R];
+            for (int b = r; b < kLineM / 16; b += R) {
+                float2 z[R];
 #pragma unroll
-            for (int q = 0; q < R; q++)
-                z[q] = lbuf[q * PF2 + 16 * b + t];
-            SmallDft<R>::run(z);
+                for (int q = 0; q < R; q++)
+                    z[q] = lbuf[q * PF2 + 16 * b + t];
+                SmallDft<R>::run(z);
 #pragma unroll
-            for (int q = 0; q < R; q++)
-                lbuf[q * PF2 + 16 * b + t] = z[q];
+                for (int q = 0; q < R; q++)
+                    lbuf[q * PF2 + 16 * b + t] = z[q];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < E; m++)
+                v[m] = buf[t + T * m];
         }
-        __syncthreads();
-#pragma unroll
-        for (int m = 0; m < E; m++)
-            v[m] = buf[t + T * m];
     };
 
     // pass 0: frequency -> space (the inverse as conj(forward(conj))) and
