@@ -887,6 +887,10 @@ def large_warmstart(args, plan, frame_dev):
         est, _ = WS.rl_planes(plan, views, k, init=init)
         return est
 
+    # how well the network fits its own training targets (8 training planes)
+    fit_views = frame_dev[:, z_train:z_train + 8].contiguous()
+    fit_ref, _ = WS.rl_planes(plan, fit_views, target_its)
+    fit_err = WS.rel_l2_planes(tiled_guess(fit_views), fit_ref.contiguous())
     tune_views = frame_dev[:, z_tune:z_tune + 8].contiguous()
     test_views = frame_dev[:, z_test:z_test + 16].contiguous()
     tune_ref, _ = WS.rl_planes(plan, tune_views, N_RL)
@@ -911,6 +915,7 @@ def large_warmstart(args, plan, frame_dev):
             "value": t_warm, "plain_rl50_ms": t_plain, "speedup": t_plain / t_warm, "k": k,
             "rel_l2_vs_rl50": {"max": float(err.max()), "mean": float(err.mean()), "tolerance": TOL},
             "k_search": {str(a): b for a, b in k_errors.items()}, "network_ms_per_16_planes": t_net,
+            "network_vs_training_targets_rel_l2": float(np.max(fit_err)),
             "training": {"planes": n_train, "crops": n_crops, "crop": CROP, "epochs": args.large_epochs,
                          "target_rl_iterations": target_its,
                          "seconds": t_train, "loss_per_epoch": hist, "data_seconds": t_data},

@@ -549,6 +549,10 @@ __global__ void __launch_bounds__(CW * 32, FMVD_COL_MIN_BLOCKS) col_pass_w(const
     const int p = blockIdx.y;
     const int x0 = blockIdx.x * FC;
     float2 *C = a.C + (size_t)p * H * W + x0;
+    // this block's slice of the spectrum (contiguous in the launch layout)
+    // is brought into L2 while the tile loads and the first transform runs
+    if (threadIdx.x == 0)
+        bulk_prefetch_l2(a.spec + (size_t)blockIdx.x * E * NT, (uint32_t)(E * NT * sizeof(float2)));
 
     if constexpr (T == 32 && FC == 8) {
         static_assert(H == 1024, "the interleaved tile path is the 1024-point column transform");
@@ -898,6 +902,10 @@ __global__ void __launch_bounds__(R * 32, 16 / R) col_pass_r(const ColArgs a)
     const int W = a.W;
     const int p = blockIdx.y;
     float2 *C = a.C + (size_t)p * H * W + 2 * blockIdx.x;
+    // this block's slice of the spectrum (contiguous in the launch layout)
+    // is brought into L2 while the tile loads and the first transform runs
+    if (threadIdx.x == 0)
+        bulk_prefetch_l2(a.spec + (size_t)blockIdx.x * E * NT, (uint32_t)(E * NT * sizeof(float2)));
 #pragma unroll 8
     for (int i = 0; i < 2 * H / NT; i++) {
         const int u = threadIdx.x + i * NT;
