@@ -52,6 +52,16 @@ __device__ __forceinline__ int clamp_src(int i, int n, int border)
     return i < n + border ? c : 0;
 }
 
+// Programmatic dependent launch.  Every pass lets the next kernel of its
+// stream launch as soon as all of its own blocks have started
+// (launch_dependents), and waits for the previous kernel to complete, with
+// its writes visible, before it reads anything an earlier kernel produced
+// (dependency_wait).  Work on constant operands (weights, spectra) may run
+// before the wait, so the next pass's blocks set up while the tail of the
+// previous one finishes.  Launched without the attribute, both are no-ops.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Requests the 128-byte line holding p into L1 (no result, no wait).
 __device__ __forceinline__ void prefetch_l1(const void *p)
 {
@@ -296,6 +306,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
     constexpr bool prefetch = SMEM && MODE != ROW_INIT;
     uint64_t *bar = &bars[gi];
     uint64_t *ebar = &ebars[MODE == ROW_UPDATE ? gi : 0];
+    pdl_launch_dependents();
     if (prefetch || MODE == ROW_UPDATE) {
         if (t == 0) {
             mbar_init(bar, 1);
@@ -305,22 +316,21 @@ __global__ void __launch_bounds__(kRowWarps * 32, FMVD_ROW_MIN_BLOCKS) row_pass_
         }
         __syncwarp();
     }
-    if (prefetch) {
-        if (t == 0) {
-            const int es = a.d.bits == 16 ? 2 : 1;
-            if (MODE == ROW_UPDATE) {
-                const uint32_t wb = a.d.dataW * sizeof(float);
-                mbar_arrive_expect_tx(bar, wb);
-                bulk_load(pf, work.wrow, wb, bar);
-            } else {
-                const uint32_t rb = a.d.dataW * es;
-                const uint32_t rs = (rb + 15) & ~15u;
-                mbar_arrive_expect_tx(bar, work.has1 ? 2 * rb : rb);
-                bulk_load(pf, work.src0, rb, bar);
-                if (work.has1)
-                    bulk_load(pf + rs, work.src1, rb, bar);
-            }
-        }
+    if (prefetch && MODE == ROW_UPDATE && t == 0) {
+        // the weight row is a plan constant: requested before the wait
+        const uint32_t wb = a.d.dataW * sizeof(float);
+        mbar_arrive_expect_tx(bar, wb);
+        bulk_load(pf, work.wrow, wb, bar);
+    }
+    pdl_wait();
+    if (prefetch && MODE == ROW_DIVIDE && t == 0) {
+        const int es = a.d.bits == 16 ? 2 : 1;
+        const uint32_t rb = a.d.dataW * es;
+        const uint32_t rs = (rb + 15) & ~15u;
+        mbar_arrive_expect_tx(bar, work.has1 ? 2 * rb : rb);
+        bulk_load(pf, work.src0, rb, bar);
+        if (work.has1)
+            bulk_load(pf + rs, work.src1, rb, bar);
     }
 
     // One copy of the transform code serves both directions: the inverse is
@@ -551,8 +561,10 @@ __global__ void __launch_bounds__(CW * 32, FMVD_COL_MIN_BLOCKS) col_pass_w(const
     float2 *C = a.C + (size_t)p * H * W + x0;
     // this block's slice of the spectrum (contiguous in the launch layout)
     // is brought into L2 while the tile loads and the first transform runs
+    pdl_launch_dependents();
     if (threadIdx.x == 0)
         bulk_prefetch_l2(a.spec + (size_t)blockIdx.x * E * NT, (uint32_t)(E * NT * sizeof(float2)));
+    pdl_wait();
 
     if constexpr (T == 32 && FC == 8) {
         static_assert(H == 1024, "the interleaved tile path is the 1024-point column transform");
@@ -724,24 +736,28 @@ __global__ void __launch_bounds__(R * 32, 16 / R) row_pass_r(const RowArgs a)
     RowWork<MODE, BITS, NOOUT, SMEM, false> work(a, p, y);
 
     // operand rows staged by bulk copies, issued now by one thread per row
+    // (the weight row, a plan constant, before the dependency wait)
     constexpr bool staged = SMEM && MODE != ROW_INIT;
     __shared__ __align__(8) uint64_t sbar[2];
     const uint32_t rb = a.d.dataW * (MODE == ROW_UPDATE ? (uint32_t)sizeof(float) : (BITS == 8 ? 1u : 2u));
     const uint32_t rs = (rb + 15) & ~15u;
     char *const st = reinterpret_cast<char *>(smem) + sizeof(float2) * 2 * R * PF2 +
                      (size_t)h * (MODE == ROW_UPDATE ? rs : 2 * rs);
+    pdl_launch_dependents();
     if (staged && threadIdx.x == 16 * h) {
         mbar_init(&sbar[h], 1);
         mbar_fence_init();
         if (MODE == ROW_UPDATE) {
             mbar_arrive_expect_tx(&sbar[h], rb);
             bulk_load(st, work.wrow, rb, &sbar[h]);
-        } else {
-            mbar_arrive_expect_tx(&sbar[h], work.has1 ? 2 * rb : rb);
-            bulk_load(st, work.src0, rb, &sbar[h]);
-            if (work.has1)
-                bulk_load(st + rs, work.src1, rb, &sbar[h]);
         }
+    }
+    pdl_wait();
+    if (staged && MODE == ROW_DIVIDE && threadIdx.x == 16 * h) {
+        mbar_arrive_expect_tx(&sbar[h], work.has1 ? 2 * rb : rb);
+        bulk_load(st, work.src0, rb, &sbar[h]);
+        if (work.has1)
+            bulk_load(st + rs, work.src1, rb, &sbar[h]);
     }
 
     // the radix-R step across the row's R groups, v[m] <- sum_j (group j's
@@ -904,8 +920,10 @@ __global__ void __launch_bounds__(R * 32, 16 / R) col_pass_r(const ColArgs a)
     float2 *C = a.C + (size_t)p * H * W + 2 * blockIdx.x;
     // this block's slice of the spectrum (contiguous in the launch layout)
     // is brought into L2 while the tile loads and the first transform runs
+    pdl_launch_dependents();
     if (threadIdx.x == 0)
         bulk_prefetch_l2(a.spec + (size_t)blockIdx.x * E * NT, (uint32_t)(E * NT * sizeof(float2)));
+    pdl_wait();
 #pragma unroll 8
     for (int i = 0; i < 2 * H / NT; i++) {
         const int u = threadIdx.x + i * NT;
@@ -1230,6 +1248,29 @@ int rl_col_warps(int H, int W, int requested)
 
 size_t rl_spectrum_elems(int H, int W) { return (size_t)H * W; }
 
+// Launch of an RL pass with programmatic dependent launch on stream s (the
+// pass's blocks may start while the previous kernel of the stream finishes;
+// the pass waits for it before reading its results).  Falls back to a plain
+// launch if the attribute is refused.
+template <typename A>
+static void launch_pass(void (*kern)(const A), dim3 grid, dim3 block, size_t smem, cudaStream_t s, const A &args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, kern, args) != cudaSuccess) {
+        cudaGetLastError();  // clear the refusal; launch without the attribute
+        kern<<<grid, block, smem, s>>>(args);
+    }
+}
+
 // Dynamic shared memory above 48 KB needs an opt-in per function and device.
 template <typename K>
 static void configure_smem(K kern, size_t bytes, unsigned &mask)
@@ -1327,7 +1368,7 @@ static void launch_row(const RowArgs &a0, cudaStream_t s)
         }
         configure_smem(kern, 200 * 1024, *m);
         dim3 grid((a.d.H + kRowWarps * G - 1) / (kRowWarps * G), a.b.npairs);
-        kern<<<grid, kRowWarps * 32, smem, s>>>(a);
+        launch_pass(kern, grid, dim3(kRowWarps * 32), smem, s, a);
     } else {
         constexpr int R = W / kLineM;
         static_assert(W % kLineM == 0 && R >= 3 && R <= 8, "rows above 1024 are 3..8 sub-lines of 512");
@@ -1351,7 +1392,7 @@ static void launch_row(const RowArgs &a0, cudaStream_t s)
             pick_row_r<R, MODE, true>(a, sm, kern, m);
         configure_smem(kern, 200 * 1024, *m);
         dim3 grid(a.d.H / 2, a.b.npairs);
-        kern<<<grid, R * 32, smem, s>>>(a);
+        launch_pass(kern, grid, dim3(R * 32), smem, s, a);
     }
     g_launches++;
 }
@@ -1367,7 +1408,7 @@ static void launch_col_w(const ColArgs &a, int npairs, cudaStream_t s)
     static unsigned mask = 0;
     configure_smem(kern, smem, mask);
     dim3 grid(a.W / FC, npairs);
-    kern<<<grid, CW * 32, smem, s>>>(a);
+    launch_pass(kern, grid, dim3(CW * 32), smem, s, a);
 }
 
 template <int H>
@@ -1388,7 +1429,7 @@ static void launch_col(const ColArgs &a, int npairs, int cw, int radix_step, cud
         static unsigned mask[2] = {0, 0};
         configure_smem(kern, smem, mask[sums ? 1 : 0]);
         dim3 grid(a.W / 2, npairs);
-        kern<<<grid, R * 32, smem, s>>>(a);
+        launch_pass(kern, grid, dim3(R * 32), smem, s, a);
     }
     g_launches++;
 }
