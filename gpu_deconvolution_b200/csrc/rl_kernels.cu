@@ -904,9 +904,14 @@ __device__ __forceinline__ void col_fft_512(float2 *v, const TW &tw, uint32_t wb
 
 // Column pass for H = R * 512: R warps, two columns per block (half-warp cc
 // of warp r is group r of column cc).  Spectrum in launch layout: block bx,
-// register m, thread tid at spec[(bx * 32 + m) * (32 R) + tid].
+// register m, thread tid at spec[(bx * 32 + m) * (32 R) + tid].  Resident
+// blocks per SM: 16 / R, except 4 (not 5) for R = 3, where the register cap of
+// five blocks spills and four run 2 % faster.
+template <int R>
+constexpr int col_r_blocks() { return R == 3 ? 4 : 16 / R; }
+
 template <int R, bool DSTEP>
-__global__ void __launch_bounds__(R * 32, 16 / R) col_pass_r(const ColArgs a)
+__global__ void __launch_bounds__(R * 32, col_r_blocks<R>()) col_pass_r(const ColArgs a)
 {
     using WF = WarpFft<kLineM>;
     static_assert(WF::T == 16 && WF::E == 32, "sub-lines are 512-point half-warp transforms");
