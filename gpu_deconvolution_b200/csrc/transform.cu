@@ -33,13 +33,19 @@ namespace fmvd {
 namespace {
 
 constexpr int TX = 32, TY = 8;  // target tile
+#ifndef FMVD_RESAMPLE_STACK
+#define FMVD_RESAMPLE_STACK 16
+#endif
+constexpr int kMaxStack = FMVD_RESAMPLE_STACK;  // target planes per CTA, at most
 
 struct Mat {
     float m[12];
 };
 
-// rx = m0 x + m1 y + m2 z + m3 (fmvd_transform.impl.cu:41-43), same evaluation order
-__device__ __forceinline__ void apply(const Mat &M, int x, int y, int z, float &rx, float &ry, float &rz)
+// rx = m0 x + m1 y + m2 z + m3 (fmvd_transform.impl.cu:41-43), same evaluation
+// order; z may be passed as the float it converts to (a whole number)
+template <typename Z>
+__device__ __forceinline__ void apply(const Mat &M, int x, int y, Z z, float &rx, float &ry, float &rz)
 {
     rx = M.m[0] * x + M.m[1] * y + M.m[2] * z + M.m[3];
     ry = M.m[4] * x + M.m[5] * y + M.m[6] * z + M.m[7];
@@ -49,23 +55,41 @@ __device__ __forceinline__ void apply(const Mat &M, int x, int y, int z, float &
 // Texel index and 1/256-quantised weight along one axis for source position r
 // (the reference fetches at r + 0.5 in unnormalised texture coordinates; the
 // filter works at xB = coordinate - 0.5).  The fractional part is rounded to
-// the nearest 1/256, halves up.
+// the nearest 1/256, halves up: q = floor((xB) * 256 + 0.5) in 1/256 texels,
+// texel q >> 8 (a floor, also below zero), weight (q mod 256) / 256.
 __device__ __forceinline__ void tex_axis(float r, int &i, float &a)
 {
     // the reference forms r + 0.5 in double and converts to float: the exact
     // sum rounded once to float, which is what one float addition gives
     const float u = __fadd_rn(r, 0.5f);
-    const float fx = (u - 0.5f) * 256.0f;
-    const float q = floorf(fx + 0.5f);
-    const float fi = floorf(q * (1.0f / 256.0f));
-    i = (int)fi;
-    a = (q - fi * 256.0f) * (1.0f / 256.0f);
+    const float xb = __fsub_rn(u, 0.5f);
+    // xb * 256 is exact, so the fused form rounds the same sum as
+    // (xb * 256) + 0.5 would; one conversion (to int, rounding down) instead
+    // of two floors and a conversion
+    const int q = __float2int_rd(__fmaf_rn(xb, 256.0f, 0.5f));
+    i = q >> 8;
+    // (q & 255) / 256 exactly: those bits placed as the lowest mantissa bits
+    // of 2^15 (whose unit in the last place is 1/256), then 2^15 taken away
+    a = __int_as_float(0x47000000 | (q & 255)) - 32768.0f;
 }
 
+// A sample as a float: the integer value is placed in the low mantissa bits
+// of 2^23 and 2^23 taken away (exact for values below 2^23), so the
+// conversion uses the FP32 pipe instead of the conversion unit.
 template <typename S>
-__device__ __forceinline__ float to_sample_float(S v, float inv)
+__device__ __forceinline__ float sample_value(S v)
 {
-    return (float)v * inv;
+    return __int_as_float(0x4B000000 | (uint32_t)v) - 8388608.0f;
+}
+
+// Trilinear blend of the corner samples t[c] (c = x + 2 y + 4 z offsets)
+// with the upper-corner weights ax, ay, az, in sample units; the texture's
+// normalised value is this times 1 / (2^bits - 1).
+__device__ __forceinline__ float blend(const float *t, float ax, float ay, float az)
+{
+    const float bx0 = 1.f - ax, by0 = 1.f - ay, bz0 = 1.f - az;
+    return bz0 * (by0 * (bx0 * t[0] + ax * t[1]) + ay * (bx0 * t[2] + ax * t[3])) +
+           az * (by0 * (bx0 * t[4] + ax * t[5]) + ay * (bx0 * t[6] + ax * t[7]));
 }
 
 template <typename S, int BITS>
@@ -82,7 +106,10 @@ __device__ __forceinline__ S quantise(float v)
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-template <typename S, int BITS>
+// Output of a resampler launch: target samples, the float blend, or both.
+constexpr int kOutSamples = 1, kOutFloat = 2;
+
+template <typename S, int BITS, int OUT>
 __global__ void __launch_bounds__(TX *TY) resample_tma(const __grid_constant__ CUtensorMap tmap,
                                                        const S *__restrict__ src, int w, int h, int d, size_t pitch,
                                                        int tw, int th, int z0, int nz, int kz, const Mat M, int bx,
@@ -91,69 +118,131 @@ __global__ void __launch_bounds__(TX *TY) resample_tma(const __grid_constant__ C
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar;
-    S *brick = reinterpret_cast<S *>(smem_raw);
+    __shared__ int origin[3];
+    // 0: no brick (every texel from global memory); 1: brick, each load
+    // checked against it; 2: brick holding every texel of the tile stack
+    __shared__ int mode;
+    const S *brick = reinterpret_cast<const S *>(smem_raw);
     constexpr int XALIGN = 16 / sizeof(S);
     // this CTA: a TX x TY tile of the kz target planes zb .. zb + kz - 1
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, zb = z0 + blockIdx.z * kz;
     const int zn = min(kz, z0 + nz - zb);
     const int tid = threadIdx.x;
 
-    // brick origin: minimum over the corners of the tile stack, one texel of slack
-    float mn[3] = {3.4e38f, 3.4e38f, 3.4e38f};
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
+    if (tid < 32) {
+        // lane c (mod 8): corner c of the tile stack.  Each source coordinate
+        // is monotonic in x, y and z separately (an affine map evaluated with
+        // monotonic roundings), and so are the texel indices, so the corners
+        // bound every index of the stack.
+        const int c = tid & 7;
         float r[3];
-        apply(M, x0 + (c & 1) * (TX - 1), y0 + ((c >> 1) & 1) * (TY - 1), zb + (c >> 2) * (zn - 1), r[0], r[1], r[2]);
+        apply(M, x0 + (c & 1) * (TX - 1), y0 + ((c >> 1) & 1) * (TY - 1), (float)(zb + (c >> 2) * (zn - 1)), r[0],
+              r[1], r[2]);
+        float mn[3] = {r[0], r[1], r[2]};
 #pragma unroll
-        for (int k = 0; k < 3; k++)
-            mn[k] = fminf(mn[k], r[k]);
+        for (int o = 1; o < 8; o <<= 1)
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                mn[k] = fminf(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+        // brick origin: one texel below the footprint, x rounded down to the
+        // 16-byte boundary a TMA copy needs
+        int ox = (int)floorf(mn[0]) - 1;
+        ox = (ox >= 0) ? (ox / XALIGN) * XALIGN : -(((-ox) + XALIGN - 1) / XALIGN) * XALIGN;
+        const int oy = (int)floorf(mn[1]) - 1;
+        const int oz = (int)floorf(mn[2]) - 1;
+        // the corners' texels inside the brick with one texel to spare on
+        // each side (room for a different rounding of the same coordinate)
+        int ix, iy, iz;
+        float a;
+        tex_axis(r[0], ix, a);
+        tex_axis(r[1], iy, a);
+        tex_axis(r[2], iz, a);
+        const bool inside = ix - ox >= 1 && ix - ox + 2 < bx && iy - oy >= 1 && iy - oy + 2 < by && iz - oz >= 1 &&
+                            iz - oz + 2 < bz;
+        const bool all_inside = __all_sync(0xffffffffu, inside);
+        if (tid == 0) {
+            origin[0] = ox;
+            origin[1] = oy;
+            origin[2] = oz;
+            const uint32_t bar_a = smem_u32(&bar);
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            const uint32_t bytes = (uint32_t)(bx * by * bz * sizeof(S));
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes) : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+                    smem_u32(smem_raw)),
+                "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(ox), "r"(oy), "r"(oz), "r"(bar_a)
+                : "memory");
+            // bounded wait for the brick (phase 0), by this thread alone: the
+            // others wait at the block barrier below, where they take no issue
+            // slots, and the barrier orders the brick's arrival before their
+            // reads
+            uint32_t done = 0;
+            for (int spin = 0; spin < (1 << 22) && !done; spin++) {
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+                    "selp.u32 %0, 1, 0, p;\n\t}"
+                    : "=r"(done)
+                    : "r"(bar_a)
+                    : "memory");
+                if (!done && spin > 64)
+                    __nanosleep(64);
+            }
+            mode = done ? (all_inside ? 2 : 1) : 0;
+            if (!done)
+                atomicExch(status, 1);
+        }
     }
-    int ox = (int)floorf(mn[0]) - 1;
-    ox = (ox >= 0) ? (ox / XALIGN) * XALIGN : -(((-ox) + XALIGN - 1) / XALIGN) * XALIGN;
-    const int oy = (int)floorf(mn[1]) - 1;
-    const int oz = (int)floorf(mn[2]) - 1;
-
-    const uint32_t bar_a = smem_u32(&bar);
-    if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    const uint32_t bytes = (uint32_t)(bx * by * bz * sizeof(S));
-    if (tid == 0) {
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes) : "memory");
-        asm volatile(
-            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
-                smem_u32(brick)),
-            "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(ox), "r"(oy), "r"(oz), "r"(bar_a)
-            : "memory");
-    }
-    // bounded wait for the brick (phase 0)
-    uint32_t done = 0;
-    for (int spin = 0; spin < (1 << 22) && !done; spin++) {
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(bar_a)
-            : "memory");
-        if (!done && spin > 64)
-            __nanosleep(64);
-    }
-    const bool have_brick = done != 0;
-    if (!have_brick && tid == 0)
-        atomicExch(status, 1);
+    __syncthreads();  // the origin and mode are written and the brick has landed (or the wait gave up)
+    const int ox = origin[0], oy = origin[1], oz = origin[2];
+    const int md = mode;
 
     const int x = x0 + (tid % TX), y = y0 + (tid / TX);
     if (x >= tw || y >= th)
         return;
     const float inv = 1.0f / (float)((1 << BITS) - 1);
+    const size_t plane = (size_t)th * tw;
+    const size_t first = ((size_t)(zb - z0) * th + y) * tw + x;
+    S *o = (OUT & kOutSamples) ? out + first : nullptr;
+    float *of = (OUT & kOutFloat) ? outf + first : nullptr;
+    const auto emit = [&](float raw) {
+        if constexpr ((OUT & kOutSamples) != 0) {
+            *o = quantise<S, BITS>(raw * inv);
+            o += plane;
+        }
+        if constexpr ((OUT & kOutFloat) != 0) {
+            *of = raw;
+            of += plane;
+        }
+    };
+    float zf = (float)zb;  // the target plane as a float: whole numbers, exact
+    if (md == 2) {
+        // every texel of the stack is in the brick: no per-voxel checks
+        const int sy = bx, sz = bx * by;
 #pragma unroll 2
-    for (int k = 0; k < zn; k++) {
-        const int z = zb + k;
+        for (int k = 0; k < zn; k++, zf += 1.0f) {
+            float rx, ry, rz;
+            apply(M, x, y, zf, rx, ry, rz);
+            int ix, iy, iz;
+            float ax, ay, az;
+            tex_axis(rx, ix, ax);
+            tex_axis(ry, iy, ay);
+            tex_axis(rz, iz, az);
+            const S *b0 = brick + ((iz - oz) * by + (iy - oy)) * bx + (ix - ox);
+            float t[8];
+#pragma unroll
+            for (int c = 0; c < 8; c++)
+                t[c] = sample_value(b0[(c >> 2) * sz + ((c >> 1) & 1) * sy + (c & 1)]);
+            emit(blend(t, ax, ay, az));
+        }
+        return;
+    }
+#pragma unroll 1
+    for (int k = 0; k < zn; k++, zf += 1.0f) {
         float rx, ry, rz;
-        apply(M, x, y, z, rx, ry, rz);
+        apply(M, x, y, zf, rx, ry, rz);
         int ix, iy, iz;
         float ax, ay, az;
         tex_axis(rx, ix, ax);
@@ -161,27 +250,21 @@ __global__ void __launch_bounds__(TX *TY) resample_tma(const __grid_constant__ C
         tex_axis(rz, iz, az);
         const int lx = ix - ox, ly = iy - oy, lz = iz - oz;
         float t[8];
-        if (have_brick && lx >= 0 && lx + 1 < bx && ly >= 0 && ly + 1 < by && lz >= 0 && lz + 1 < bz) {
+        if (md == 1 && (unsigned)lx < (unsigned)(bx - 1) && (unsigned)ly < (unsigned)(by - 1) &&
+            (unsigned)lz < (unsigned)(bz - 1)) {
             const S *b0 = brick + (lz * by + ly) * bx + lx;
 #pragma unroll
             for (int c = 0; c < 8; c++)
-                t[c] = to_sample_float(b0[((c >> 2) * by + ((c >> 1) & 1)) * bx + (c & 1)], inv);
+                t[c] = sample_value(b0[((c >> 2) * by + ((c >> 1) & 1)) * bx + (c & 1)]);
         } else {
 #pragma unroll
             for (int c = 0; c < 8; c++) {
                 const int sx = ix + (c & 1), sy = iy + ((c >> 1) & 1), sz = iz + (c >> 2);
                 const bool in = sx >= 0 && sx < w && sy >= 0 && sy < h && sz >= 0 && sz < d;
-                t[c] = in ? to_sample_float(__ldg(src + ((size_t)sz * h + sy) * pitch + sx), inv) : 0.f;
+                t[c] = in ? sample_value(__ldg(src + ((size_t)sz * h + sy) * pitch + sx)) : 0.f;
             }
         }
-        const float bx0 = 1.f - ax, by0 = 1.f - ay, bz0 = 1.f - az;
-        const float v = bz0 * (by0 * (bx0 * t[0] + ax * t[1]) + ay * (bx0 * t[2] + ax * t[3])) +
-                        az * (by0 * (bx0 * t[4] + ax * t[5]) + ay * (bx0 * t[6] + ax * t[7]));
-        const size_t oi = ((size_t)(z - z0) * th + y) * tw + x;
-        if (out)
-            out[oi] = quantise<S, BITS>(v);
-        if (outf)
-            outf[oi] = v * (float)((1 << BITS) - 1);
+        emit(blend(t, ax, ay, az));
     }
 }
 
@@ -244,19 +327,26 @@ bool resample_device(int bits, const void *d_src, size_t pitch, int w, int h, in
     memcpy(M.m, h_inverse, sizeof(M.m));
     const int xalign = (int)(16 / es);
     // box covering the footprint of a stack of kz tiles: extent + 2 texels
-    // for the filter and slack, plus the alignment of the x origin; kz is the
-    // deepest stack (8, 4, 2 or 1 target planes) whose box fits
+    // for the filter and slack, one more so that every texel of the stack is
+    // in the brick with one to spare, plus the alignment of the x origin; kz
+    // is the deepest stack (8, 4, 2 or 1 target planes) whose box fits
     int box[3] = {0, 0, 0};
-    int kz = 8;
+    int kz = kMaxStack;
     size_t smem = 0;
     bool boxes_ok = false;
     for (; kz >= 1; kz /= 2) {
         for (int a = 0; a < 3; a++) {
             const float ext = fabsf(M.m[4 * a]) * (TX - 1) + fabsf(M.m[4 * a + 1]) * (TY - 1) +
                               fabsf(M.m[4 * a + 2]) * (kz - 1);
-            box[a] = ceil_i(ext) + 4;
+            box[a] = ceil_i(ext) + 5;
         }
         box[0] = ((box[0] + xalign - 1 + xalign - 1) / xalign) * xalign;
+        // shared-memory banks: a brick row is 16 bytes times an odd number
+        // and a plane an odd number of rows, so lanes that step through rows
+        // or planes (rotated views) spread over 8 banks instead of 2 or 4
+        if ((box[0] / xalign) % 2 == 0)
+            box[0] += xalign;
+        box[1] |= 1;
         smem = (size_t)box[0] * box[1] * box[2] * es;
         boxes_ok = box[0] <= 256 && box[1] <= 256 && box[2] <= 256 && smem <= 96 * 1024;
         if (boxes_ok)
@@ -279,34 +369,41 @@ bool resample_device(int bits, const void *d_src, size_t pitch, int w, int h, in
                                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         use_tma = (r == CUDA_SUCCESS);
     }
-    if (!use_tma) {
-        // no brick fits (extreme scaling): every voxel takes the direct path
-        box[0] = box[1] = box[2] = 0;
-    }
     dim3 grid((tw + TX - 1) / TX, (th + TY - 1) / TY, (nz + kz - 1) / kz);
-    const size_t shm = use_tma ? smem : 0;
+    if (!use_tma) {  // no brick fits (extreme scaling): every voxel takes the direct path
+        resample_direct(bits, d_src, pitch, w, h, d, tw, th, z0, nz, h_inverse, d_out, d_outf, s);
+        return FMVD_CHECK(cudaGetLastError());
+    }
+    const int mode = (d_out ? kOutSamples : 0) | (d_outf ? kOutFloat : 0);
+    if (mode == 0)
+        return true;
+    const auto launch = [&](auto kern, auto *src_typed, auto *out_typed) {
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, TX * TY, smem, s>>>(tmap, src_typed, w, h, d, pitch, tw, th, z0, nz, kz, M, box[0], box[1],
+                                         box[2], out_typed, d_outf, d_status);
+        rl_count_launch(1);
+    };
     if (bits == 16) {
-        auto k = resample_tma<unsigned short, 16>;
-        if (shm > 48 * 1024)
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-        if (use_tma) {
-            k<<<grid, TX * TY, shm, s>>>(tmap, (const unsigned short *)d_src, w, h, d, pitch, tw, th, z0, nz, kz, M,
-                                         box[0], box[1], box[2], (unsigned short *)d_out, d_outf, d_status);
-            rl_count_launch(1);
-        } else {
-            resample_direct(bits, d_src, pitch, w, h, d, tw, th, z0, nz, h_inverse, d_out, d_outf, s);
-        }
+        using S = unsigned short;
+        const S *sp = (const S *)d_src;
+        S *op = (S *)d_out;
+        if (mode == kOutSamples)
+            launch(resample_tma<S, 16, kOutSamples>, sp, op);
+        else if (mode == kOutFloat)
+            launch(resample_tma<S, 16, kOutFloat>, sp, op);
+        else
+            launch(resample_tma<S, 16, kOutSamples | kOutFloat>, sp, op);
     } else {
-        auto k = resample_tma<unsigned char, 8>;
-        if (shm > 48 * 1024)
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-        if (use_tma) {
-            k<<<grid, TX * TY, shm, s>>>(tmap, (const unsigned char *)d_src, w, h, d, pitch, tw, th, z0, nz, kz, M,
-                                         box[0], box[1], box[2], (unsigned char *)d_out, d_outf, d_status);
-            rl_count_launch(1);
-        } else {
-            resample_direct(bits, d_src, pitch, w, h, d, tw, th, z0, nz, h_inverse, d_out, d_outf, s);
-        }
+        using S = unsigned char;
+        const S *sp = (const S *)d_src;
+        S *op = (S *)d_out;
+        if (mode == kOutSamples)
+            launch(resample_tma<S, 8, kOutSamples>, sp, op);
+        else if (mode == kOutFloat)
+            launch(resample_tma<S, 8, kOutFloat>, sp, op);
+        else
+            launch(resample_tma<S, 8, kOutSamples | kOutFloat>, sp, op);
     }
     return FMVD_CHECK(cudaGetLastError());
 }
@@ -345,16 +442,14 @@ __global__ void resample_direct_kernel(const S *__restrict__ src, int w, int h, 
     for (int c = 0; c < 8; c++) {
         const int sx = ix + (c & 1), sy = iy + ((c >> 1) & 1), sz = iz + (c >> 2);
         const bool in = sx >= 0 && sx < w && sy >= 0 && sy < h && sz >= 0 && sz < d;
-        t[c] = in ? to_sample_float(__ldg(src + ((size_t)sz * h + sy) * pitch + sx), inv) : 0.f;
+        t[c] = in ? sample_value(__ldg(src + ((size_t)sz * h + sy) * pitch + sx)) : 0.f;
     }
-    const float bx0 = 1.f - ax, by0 = 1.f - ay, bz0 = 1.f - az;
-    const float v = bz0 * (by0 * (bx0 * t[0] + ax * t[1]) + ay * (bx0 * t[2] + ax * t[3])) +
-                    az * (by0 * (bx0 * t[4] + ax * t[5]) + ay * (bx0 * t[6] + ax * t[7]));
+    const float raw = blend(t, ax, ay, az);
     const size_t oi = ((size_t)blockIdx.z * th + y) * tw + x;
     if (out)
-        out[oi] = quantise<S, BITS>(v);
+        out[oi] = quantise<S, BITS>(raw * inv);
     if (outf)
-        outf[oi] = v * (float)((1 << BITS) - 1);
+        outf[oi] = raw;
 }
 
 void resample_direct(int bits, const void *d_src, size_t pitch, int w, int h, int d, int tw, int th, int z0, int nz,

@@ -113,6 +113,39 @@ def test_transform_large_frame_vs_texture_unit():
         check_vs_texture_unit(got, ref, src, m, frame, 16)
 
 
+@pytest.mark.parametrize("bits", [16, 8])
+def test_transform_float_frame_vs_oracle(bits):
+    """The float frame (d_outf: the blend in sample units before
+    quantisation) against the oracle's unquantised value: within float
+    rounding where the 1/256 weights agree, within one weight step per axis
+    elsewhere; and the sample frame written beside it is exactly the float
+    frame quantised, (sample)(v / (2^bits - 1) * 2^bits + 0.5) in float."""
+    import torch
+    src = volume(bits=bits, shape=(30, 40, 44))
+    d, h, w = src.shape
+    frame = (50, 40, 44)
+    pitch = api.source_pitch(bits, w)
+    padded = np.zeros((d, h, pitch), src.dtype)
+    padded[:, :, :w] = src
+    dev = torch.from_numpy(padded.view(np.int16) if bits == 16 else padded).cuda()
+    maxv = float((1 << bits) - 1)
+    for m in matrices(frame, src.shape):
+        out = torch.zeros(frame, dtype=torch.int16 if bits == 16 else torch.uint8, device="cuda")
+        outf = torch.zeros(frame, dtype=torch.float32, device="cuda")
+        api.transform_device(dev, pitch, w, h, d, m, frame[2], frame[1], 0, frame[0], out=out, out_f32=outf,
+                             bits=bits)
+        torch.cuda.synchronize()
+        gf = outf.cpu().numpy()
+        gs = out.cpu().numpy().view(np.uint16) if bits == 16 else out.cpu().numpy()
+        ref = O.transform_volume(src, m, *frame, bits=bits, out_float=True) * maxv
+        diff = np.abs(gf.astype(np.float64) - ref)
+        sens = O.transform_weight_sensitivity(src, m, *frame, bits=bits)
+        assert np.all(diff <= sens + 0.05), (diff - sens).max()
+        assert (diff <= 0.05).mean() > 0.98
+        q = np.floor(gf * np.float32(1.0 / maxv) * np.float32(1 << bits) + np.float32(0.5)).astype(np.int64)
+        np.testing.assert_array_equal(gs.astype(np.int64), q % (1 << bits))
+
+
 def test_transform_file_and_mask(tmp_path):
     src = volume()
     frame = (24, 20, 28)
