@@ -532,11 +532,15 @@ def run_warmstart(args):
     print(json.dumps(warmstart_result(args)), flush=True)
 
 
+K_TUNE_MARGIN = 0.9  # warm-start k is tuned to this fraction of the tolerance
+
+
 def warmstart_result(args, log=True):
     """Learned warm start (a 2-D U-Net on the tensor cores) vs plain RL-50 on
     512 x 512 planes of 4 views: train on plain RL-50 targets, tune k so that
-    warm start + RL-k is within 1e-2 relative L2 of plain RL-50 on held-out
-    planes, then time both paths to the RL-50 result on test planes."""
+    warm start + RL-k is within 0.9e-2 relative L2 of plain RL-50 on its own
+    planes, then time both paths to the RL-50 result on test planes, where the
+    tolerance is 1e-2."""
     import torch
     from gpu_deconvolution_b200 import api
     from gpu_deconvolution_b200 import warmstart as WS
@@ -563,7 +567,9 @@ def warmstart_result(args, log=True):
     fwd_f, train_f = unet_flops_per_plane(H, W, V)
     del views, targets, gt
     torch.cuda.empty_cache()
-    k, k_errors = WS.tune_k(net, plan, tv, tt, TOL,
+    # k is tuned on its own planes to 90 % of the tolerance, so that the
+    # held-out test planes (a different sample) stay within it
+    k, k_errors = WS.tune_k(net, plan, tv, tt, K_TUNE_MARGIN * TOL,
                             candidates=tuple(range(0, 13)) + (14, 16, 20, 25, 30, 40))
     kk = k if k is not None else N_RL
     # time to the RL-50 result on the test planes
@@ -579,7 +585,8 @@ def warmstart_result(args, log=True):
     line = {
         "metric": "time to the plain RL-50 result, warm start vs plain", "unit": "ms per 64 planes",
         "value": t_warm, "plain_rl50_ms": t_plain, "speedup": t_plain / t_warm, "k": k,
-        "rel_l2_vs_rl50": {"max": float(err.max()), "mean": float(err.mean()), "tolerance": TOL},
+        "rel_l2_vs_rl50": {"max": float(err.max()), "mean": float(err.mean()), "tolerance": TOL,
+                           "k_tuned_to": K_TUNE_MARGIN * TOL},
         "psnr_db": {"plain_rl50": psnr_plain, "warm": psnr_warm, "delta": psnr_warm - psnr_plain},
         "k_search": {str(a): b for a, b in k_errors.items()},
         "network_ms_per_64_planes": t_net,
@@ -899,7 +906,7 @@ def large_warmstart(args, plan, frame_dev):
     for cand in tuple(range(0, 13)) + (14, 16, 20, 25, 30, 40):
         err = float(np.max(WS.rel_l2_planes(warm(tune_views, cand).contiguous(), tune_ref)))
         k_errors[cand] = err
-        if err <= TOL:
+        if err <= K_TUNE_MARGIN * TOL:
             k = cand
             break
     kk = k if k is not None else N_RL
