@@ -7,10 +7,12 @@
 // it back plane by plane).  Here the host traffic is the source volumes in and
 // the result out: the sources are uploaded once (on a copy stream, view by
 // view, the first chunk starting on each view as it lands), then target
-// planes are processed in chunks on one stream (resample V views into a
-// device chunk, deconvolve it, write the chunk's samples), while the copy
-// stream moves the previous chunk's result to pinned staging and the host
-// thread moves it into the caller's buffer.
+// planes are processed in chunks: a resampling stream fills a device chunk
+// with the V views' planes (double-buffered, so chunk k + 1 is resampled
+// while chunk k deconvolves), the compute stream deconvolves it and writes
+// the chunk's samples, the copy stream moves the previous chunk's result to
+// pinned staging and the host thread moves it into the caller's buffer (with
+// a few helper threads: one thread copies only a few GB/s).
 #include "fmvd_b200.h"
 #include "fmvd_internal.h"
 #include "transform_kernels.h"
@@ -27,8 +29,8 @@ struct fmvd_b200_reconstructor {
     void *out[2] = {};            // chunk x th x tw samples
     void *stage[2] = {};          // pinned, chunk x th x tw samples
     int *status = nullptr;
-    cudaStream_t comp = nullptr, copy = nullptr;
-    cudaEvent_t done[2] = {}, copied[2] = {};
+    cudaStream_t comp = nullptr, copy = nullptr, rs = nullptr;
+    cudaEvent_t done[2] = {}, copied[2] = {}, resampled[2] = {};
     std::vector<cudaEvent_t> uploaded;  // per view: its source volume is on the device
 };
 
@@ -47,6 +49,8 @@ void release(fmvd_b200_reconstructor *r)
             cudaEventDestroy(r->done[i]);
         if (r->copied[i])
             cudaEventDestroy(r->copied[i]);
+        if (r->resampled[i])
+            cudaEventDestroy(r->resampled[i]);
     }
     for (cudaEvent_t e : r->uploaded)
         if (e)
@@ -56,6 +60,8 @@ void release(fmvd_b200_reconstructor *r)
         cudaStreamDestroy(r->comp);
     if (r->copy)
         cudaStreamDestroy(r->copy);
+    if (r->rs)
+        cudaStreamDestroy(r->rs);
     delete r;
 }
 
@@ -93,13 +99,15 @@ fmvd_b200_reconstructor *fmvd_b200_reconstructor_create(fmvd_b200_plan *plan, in
     bool ok = FMVD_CHECK(cudaMalloc(&r->src, (size_t)views * d * h * r->pitch * r->es)) &&
               FMVD_CHECK(cudaMalloc(&r->status, sizeof(int))) && FMVD_CHECK(cudaMemset(r->status, 0, sizeof(int))) &&
               FMVD_CHECK(cudaStreamCreateWithFlags(&r->comp, cudaStreamNonBlocking)) &&
-              FMVD_CHECK(cudaStreamCreateWithFlags(&r->copy, cudaStreamNonBlocking));
+              FMVD_CHECK(cudaStreamCreateWithFlags(&r->copy, cudaStreamNonBlocking)) &&
+              FMVD_CHECK(cudaStreamCreateWithFlags(&r->rs, cudaStreamNonBlocking));
     for (int i = 0; i < 2 && ok; i++)
         ok = FMVD_CHECK(cudaMalloc(&r->frame[i], (size_t)views * chunk * plane)) &&
              FMVD_CHECK(cudaMalloc(&r->out[i], (size_t)chunk * plane)) &&
              FMVD_CHECK(cudaMallocHost(&r->stage[i], (size_t)chunk * plane)) &&
              FMVD_CHECK(cudaEventCreateWithFlags(&r->done[i], cudaEventDisableTiming)) &&
-             FMVD_CHECK(cudaEventCreateWithFlags(&r->copied[i], cudaEventDisableTiming));
+             FMVD_CHECK(cudaEventCreateWithFlags(&r->copied[i], cudaEventDisableTiming)) &&
+             FMVD_CHECK(cudaEventCreateWithFlags(&r->resampled[i], cudaEventDisableTiming));
     r->uploaded.assign(views, nullptr);
     for (int v = 0; v < views && ok; v++)
         ok = FMVD_CHECK(cudaEventCreateWithFlags(&r->uploaded[v], cudaEventDisableTiming));
@@ -120,7 +128,7 @@ int fmvd_b200_reconstruct_host(fmvd_b200_reconstructor *r, const void *const *h_
     const size_t es = r->es;
     const size_t plane = (size_t)r->tw * r->th * es;
     const size_t vol = (size_t)r->d * r->h * r->pitch * es;
-    bool ok = FMVD_CHECK(cudaMemsetAsync(r->status, 0, sizeof(int), r->comp));
+    bool ok = FMVD_CHECK(cudaMemsetAsync(r->status, 0, sizeof(int), r->rs));
     // sources: each view d x h x w contiguous on the host -> pitched device
     // rows, on the copy stream; the first chunk resamples view v as soon as
     // view v has landed, so the upload of later views overlaps it
@@ -132,15 +140,19 @@ int fmvd_b200_reconstruct_host(fmvd_b200_reconstructor *r, const void *const *h_
     auto planes_of = [&](int k) { return r->td - k * r->chunk < r->chunk ? r->td - k * r->chunk : r->chunk; };
     for (int k = 0; k < nchunks && ok; k++) {
         const int b = k & 1, z0 = k * r->chunk, n = planes_of(k);
-        if (k >= 2)  // the copy of chunk k - 2 has read out[b]
-            ok = FMVD_CHECK(cudaStreamWaitEvent(r->comp, r->copied[b], 0));
+        if (k >= 2)  // the deconvolution of chunk k - 2 has read frame[b]
+            ok = FMVD_CHECK(cudaStreamWaitEvent(r->rs, r->done[b], 0));
         for (int v = 0; v < r->V && ok; v++)
-            ok = (k > 0 || FMVD_CHECK(cudaStreamWaitEvent(r->comp, r->uploaded[v], 0))) &&
+            ok = (k > 0 || FMVD_CHECK(cudaStreamWaitEvent(r->rs, r->uploaded[v], 0))) &&
                  fmvd::resample_device(r->bits, (const char *)r->src + v * vol, r->pitch, r->w, r->h, r->d, r->tw,
                                        r->th, z0, n, h_inverses + 12 * v,
                                        (char *)r->frame[b] + (size_t)v * r->chunk * plane, nullptr, r->status,
-                                       r->comp);
-        ok = ok && fmvd::engine_run(r->plan->eng, r->frame[b], (size_t)r->chunk * r->tw * r->th, r->out[b], n,
+                                       r->rs);
+        ok = ok && FMVD_CHECK(cudaEventRecord(r->resampled[b], r->rs));
+        if (ok && k >= 2)  // the copy of chunk k - 2 has read out[b]
+            ok = FMVD_CHECK(cudaStreamWaitEvent(r->comp, r->copied[b], 0));
+        ok = ok && FMVD_CHECK(cudaStreamWaitEvent(r->comp, r->resampled[b], 0)) &&
+             fmvd::engine_run(r->plan->eng, r->frame[b], (size_t)r->chunk * r->tw * r->th, r->out[b], n,
                                     iterations, nullptr, r->comp) &&
              FMVD_CHECK(cudaEventRecord(r->done[b], r->comp)) &&
              FMVD_CHECK(cudaStreamWaitEvent(r->copy, r->done[b], 0)) &&
@@ -150,17 +162,18 @@ int fmvd_b200_reconstruct_host(fmvd_b200_reconstructor *r, const void *const *h_
             const int pb = (k - 1) & 1;
             ok = FMVD_CHECK(cudaEventSynchronize(r->copied[pb]));
             if (ok)
-                memcpy((char *)h_out + (size_t)(k - 1) * r->chunk * plane, r->stage[pb], planes_of(k - 1) * plane);
+                fmvd::host_copy((char *)h_out + (size_t)(k - 1) * r->chunk * plane, r->stage[pb],
+                                planes_of(k - 1) * plane);
         }
     }
     if (ok) {
         const int k = nchunks - 1, b = k & 1;
         ok = FMVD_CHECK(cudaEventSynchronize(r->copied[b]));
         if (ok)
-            memcpy((char *)h_out + (size_t)k * r->chunk * plane, r->stage[b], planes_of(k) * plane);
+            fmvd::host_copy((char *)h_out + (size_t)k * r->chunk * plane, r->stage[b], planes_of(k) * plane);
     }
     int status = 0;
-    ok = ok && FMVD_CHECK(cudaStreamSynchronize(r->comp)) &&
+    ok = ok && FMVD_CHECK(cudaStreamSynchronize(r->rs)) && FMVD_CHECK(cudaStreamSynchronize(r->comp)) &&
          FMVD_CHECK(cudaMemcpy(&status, r->status, sizeof(int), cudaMemcpyDeviceToHost));
     if (ok && status) {
         fmvd::report_error("fmvd: a resampler brick load did not complete in time");
@@ -173,6 +186,7 @@ void fmvd_b200_reconstructor_destroy(fmvd_b200_reconstructor *r)
 {
     if (!r)
         return;
+    cudaStreamSynchronize(r->rs);
     cudaStreamSynchronize(r->comp);
     cudaStreamSynchronize(r->copy);
     release(r);
