@@ -80,8 +80,11 @@ def parse():
     p.add_argument("--large-target-iterations", type=int, default=40,
                    help="large workload: RL iterations of the warm-start training targets")
     p.add_argument("--train-planes", type=int, default=4000)
-    p.add_argument("--epochs", type=int, default=12)
-    p.add_argument("--target-iterations", type=int, default=42,
+    # 16 epochs on RL-48 targets: over 2 seeds x 3 targets (42, 46, 48), 16
+    # epochs kept every network within 0.9 % of RL-50 on the tuning planes at
+    # its best k, 12 epochs only half of them
+    p.add_argument("--epochs", type=int, default=16)
+    p.add_argument("--target-iterations", type=int, default=48,
                    help="warm start: RL iterations of the training targets (the network then needs 50 - this)")
     return p.parse_args()
 
@@ -533,11 +536,14 @@ def run_warmstart(args):
 
 
 K_TUNE_MARGIN = 0.9  # warm-start k is tuned to this fraction of the tolerance
+WARM_SEEDS = 3       # networks trained at most, until one meets the margin
 
 
 def warmstart_result(args, log=True):
     """Learned warm start (a 2-D U-Net on the tensor cores) vs plain RL-50 on
-    512 x 512 planes of 4 views: train on plain RL-50 targets, tune k so that
+    512 x 512 planes of 4 views: train on plain RL-N targets (N =
+    --target-iterations, a little under 50 so that k RL iterations after the
+    network's estimate land on RL-50), tune k so that
     warm start + RL-k is within 0.9e-2 relative L2 of plain RL-50 on its own
     planes, then time both paths to the RL-50 result on test planes, where the
     tolerance is 1e-2."""
@@ -553,24 +559,34 @@ def warmstart_result(args, log=True):
     t_data = time.perf_counter() - t0
     tv, tt, tg, _ = WS.training_pairs(64, H, W, V, N_RL, seed=900000, planes_per_volume=64)   # k tuning
     ev, et, eg, _ = WS.training_pairs(64, H, W, V, N_RL, seed=950000, planes_per_volume=64)   # test
-    net = WS.WarmStartNet(H, W, V, max_batch=16, seed=0)
     plan = api.DevicePlan(H, W, WS.equal_weights(H, W, V), [p.copy() for p in psfs], 0)
-    # training (timed on the device, steps of 16 planes)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    hist = WS.train(net, views, targets, epochs=args.epochs, batch=16, lr=1e-3,
-                    log=(lambda m: print(m, file=sys.stderr, flush=True)) if log else None)
-    e1.record()
-    torch.cuda.synchronize()
-    t_train = e0.elapsed_time(e1) / 1e3
-    steps = args.epochs * (n_train // 16)
     fwd_f, train_f = unet_flops_per_plane(H, W, V)
+    # Training (timed on the device, steps of 16 planes), then k tuned on its
+    # own planes to 90 % of the tolerance, so that the held-out test planes
+    # (a different sample) stay within it.  The atomics of the weight
+    # gradients make each training a little different; a network whose
+    # tuning planes do not come within the margin at any k is replaced by
+    # one trained from the next seed (model selection on the tuning planes
+    # only), up to WARM_SEEDS networks.
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_train, trained = 0.0, []
+    for seed in range(WARM_SEEDS):
+        net = WS.WarmStartNet(H, W, V, max_batch=16, seed=seed)
+        e0.record()
+        hist = WS.train(net, views, targets, epochs=args.epochs, batch=16, lr=1e-3, seed=seed,
+                        log=(lambda m: print(m, file=sys.stderr, flush=True)) if log else None)
+        e1.record()
+        torch.cuda.synchronize()
+        t_train += e0.elapsed_time(e1) / 1e3
+        k, k_errors = WS.tune_k(net, plan, tv, tt, K_TUNE_MARGIN * TOL,
+                                candidates=tuple(range(0, 13)) + (14, 16, 20, 25, 30, 40))
+        trained.append({"seed": seed, "k": k, "best_tuning_rel_l2": min(k_errors.values())})
+        if k is not None or seed == WARM_SEEDS - 1:
+            break
+        net.destroy()
+    steps = args.epochs * (n_train // 16) * len(trained)
     del views, targets, gt
     torch.cuda.empty_cache()
-    # k is tuned on its own planes to 90 % of the tolerance, so that the
-    # held-out test planes (a different sample) stay within it
-    k, k_errors = WS.tune_k(net, plan, tv, tt, K_TUNE_MARGIN * TOL,
-                            candidates=tuple(range(0, 13)) + (14, 16, 20, 25, 30, 40))
     kk = k if k is not None else N_RL
     # time to the RL-50 result on the test planes
     t_plain = WS.time_cuda(lambda: WS.rl_planes(plan, ev, N_RL))
@@ -594,10 +610,11 @@ def warmstart_result(args, log=True):
         "training": {"planes": n_train, "target_rl_iterations": args.target_iterations, "epochs": args.epochs,
                      "batch": 16, "steps": steps, "seconds": t_train,
                      "tflops": train_f * 16 * steps / t_train / 1e12, "loss_per_epoch": hist,
-                     "data_seconds": t_data},
+                     "data_seconds": t_data, "networks": trained},
         "dtype": "bf16 network (fp32 accumulation), f32 RL", "data": "synthetic",
         "config": {"workload": "learned warm start: 4 views u16 512x512 planes, 17x17 PSFs sigma 1.5x4.0, "
-                               "plain RL-50 targets, U-Net 4 levels base 32", "fft_plane": [plan.fftH, plan.fftW]},
+                               f"trained on plain RL-{args.target_iterations} targets, compared with plain RL-50, "
+                               "U-Net 4 levels base 32", "fft_plane": [plan.fftH, plan.fftW]},
     }
     plan.destroy()
     net.destroy()

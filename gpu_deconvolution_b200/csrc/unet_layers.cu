@@ -354,16 +354,47 @@ __global__ void output_grad_kernel(const bf16 *act, const float *w, int C, size_
 
 // Adam on the FP32 master parameters (bias-corrected step size lr_t).
 __global__ void adam_kernel(float *param, const float *grad, float *m, float *v, size_t n, float lr_t, float b1,
-                            float b2, float eps)
+                            float b2, float eps, const float *gscale)
 {
+    const float sc = gscale ? *gscale : 1.f;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const float g = grad[i];
+        const float g = grad[i] * sc;
         const float mi = b1 * m[i] + (1.f - b1) * g;
         const float vi = b2 * v[i] + (1.f - b2) * g * g;
         m[i] = mi;
         v[i] = vi;
         param[i] -= lr_t * mi / (sqrtf(vi) + eps);
     }
+}
+
+// Squared L2 norm of the gradient, added into *out (zeroed by the caller).
+__global__ void grad_norm2_kernel(const float *g, size_t n, float *out)
+{
+    float acc = 0.f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        acc = fmaf(g[i], g[i], acc);
+    for (int o = 16; o; o >>= 1)
+        acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0)
+        atomicAdd(out, acc);
+}
+
+// Adaptive clipping of one step: state[0] = the step's squared gradient
+// norm, state[1] = running mean of the (clipped) norms of earlier steps (0
+// before the first), state[2] = the factor Adam applies to this step's
+// gradient: limit / norm where the norm exceeds limit = factor x the running
+// mean, 0 for a non-finite norm (the step is skipped), else 1.
+__global__ void clip_scale_kernel(float *state, float factor)
+{
+    const float norm = sqrtf(state[0]);
+    if (!isfinite(norm)) {
+        state[2] = 0.f;
+        return;
+    }
+    const float mean = state[1] > 0.f ? state[1] : norm;
+    const float limit = factor * mean;
+    state[2] = norm > limit && norm > 0.f ? limit / norm : 1.f;
+    state[1] = 0.95f * mean + 0.05f * fminf(norm, limit);
 }
 
 // bf16 forward weights w[co][t][ci] and data-gradient weights
@@ -465,9 +496,17 @@ bool output_grad(const bf16 *act, const float *w, int C, size_t P, const float *
 }
 
 bool adam(float *param, const float *grad, float *m, float *v, size_t n, float lr_t, float b1, float b2, float eps,
-          cudaStream_t s)
+          cudaStream_t s, float *clip_state, float clip_factor)
 {
-    adam_kernel<<<grid_for(n), 256, 0, s>>>(param, grad, m, v, n, lr_t, b1, b2, eps);
+    if (clip_state) {
+        if (!FMVD_CHECK(cudaMemsetAsync(clip_state, 0, sizeof(float), s)))
+            return false;
+        grad_norm2_kernel<<<grid_for(n), 256, 0, s>>>(grad, n, clip_state);
+        clip_scale_kernel<<<1, 1, 0, s>>>(clip_state, clip_factor);
+        rl_count_launch(2);
+    }
+    adam_kernel<<<grid_for(n), 256, 0, s>>>(param, grad, m, v, n, lr_t, b1, b2, eps,
+                                            clip_state ? clip_state + 2 : nullptr);
     rl_count_launch(1);
     return FMVD_CHECK(cudaGetLastError());
 }

@@ -30,8 +30,12 @@ bool output_layer(const __nv_bfloat16 *act, const float *w, const float *b, int 
                   float *estimate, const float *target, float *gy, float *loss, cudaStream_t s);
 bool output_grad(const __nv_bfloat16 *act, const float *w, int C, size_t P, const float *gy, __nv_bfloat16 *g_act,
                  float *dw, float *db, cudaStream_t s);
+// One Adam step.  With clip_state (3 floats on the device, zeroed before the
+// first step) the gradient is first clipped adaptively: scaled down to
+// clip_factor x the running mean of earlier steps' norms where its L2 norm
+// exceeds that, and the step skipped where the norm is not finite.
 bool adam(float *param, const float *grad, float *m, float *v, size_t n, float lr_t, float b1, float b2, float eps,
-          cudaStream_t s);
+          cudaStream_t s, float *clip_state = nullptr, float clip_factor = 2.f);
 bool weight_copies(const float *w, int cout, int taps, int cin, __nv_bfloat16 *wf, __nv_bfloat16 *wt, cudaStream_t s);
 
 } // namespace unet

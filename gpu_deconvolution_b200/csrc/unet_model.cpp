@@ -48,6 +48,7 @@ struct Net {
     bf16 *Ea[4], *Eb[4], *P[3], *U[3], *Da[3], *Db[3];
     bf16 *gEa[4], *gEb[4], *gP[3], *gU[3], *gDa[3], *gDb[3];
     float *scale = nullptr, *gy = nullptr, *loss = nullptr;
+    float *clip = nullptr;  // adaptive gradient clipping state (3 floats)
     int *status = nullptr;
     std::vector<void *> allocs;
 };
@@ -278,7 +279,8 @@ Net *create(int H, int W, int V, int maxN, unsigned seed)
         wtotal += 2 * (size_t)l.cout * l.taps * l.cin;
     bool ok = dalloc(*n, &n->params, off) && dalloc(*n, &n->grads, off) && dalloc(*n, &n->m, off) &&
               dalloc(*n, &n->v, off) && dalloc(*n, &n->wbuf, wtotal) && dalloc(*n, &n->scale, (size_t)maxN * (kScaleParts + 1)) &&
-              dalloc(*n, &n->gy, (size_t)maxN * H * W) && dalloc(*n, &n->loss, 1) && dalloc(*n, &n->status, 1);
+              dalloc(*n, &n->gy, (size_t)maxN * H * W) && dalloc(*n, &n->loss, 1) && dalloc(*n, &n->status, 1) &&
+              dalloc(*n, &n->clip, 3);
     if (ok) {
         bf16 *w = n->wbuf;
         for (Layer &l : n->L) {
@@ -306,6 +308,7 @@ Net *create(int H, int W, int V, int maxN, unsigned seed)
     ok = ok && FMVD_CHECK(cudaMemcpy(n->params, h.data(), off * sizeof(float), cudaMemcpyHostToDevice)) &&
          FMVD_CHECK(cudaMemset(n->m, 0, off * sizeof(float))) && FMVD_CHECK(cudaMemset(n->v, 0, off * sizeof(float))) &&
          FMVD_CHECK(cudaMemset(n->grads, 0, off * sizeof(float))) && FMVD_CHECK(cudaMemset(n->status, 0, sizeof(int))) &&
+         FMVD_CHECK(cudaMemset(n->clip, 0, 3 * sizeof(float))) &&
          refresh_weights(*n, 0) && FMVD_CHECK(cudaDeviceSynchronize());
     if (!ok) {
         release(n);
@@ -345,7 +348,11 @@ bool train_step(Net *n, const unsigned short *views, size_t vs, int N, const flo
     if (ok && lr > 0.f) {
         n->step++;
         const float lr_t = lr * sqrtf(1.f - powf(b2, (float)n->step)) / (1.f - powf(b1, (float)n->step));
-        ok = adam(n->params, n->grads, n->m, n->v, n->nparams, lr_t, b1, b2, eps, s) && refresh_weights(*n, s);
+        // adaptive clipping keeps a rare outsized gradient (a loss spike
+        // that otherwise set training back by several epochs) from
+        // scattering the weights
+        ok = adam(n->params, n->grads, n->m, n->v, n->nparams, lr_t, b1, b2, eps, s, n->clip, 2.f) &&
+             refresh_weights(*n, s);
     }
     if (ok && h_loss)
         ok = FMVD_CHECK(cudaMemcpyAsync(h_loss, n->loss, sizeof(float), cudaMemcpyDeviceToHost, s)) &&

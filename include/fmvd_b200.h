@@ -197,7 +197,10 @@ int fmvd_b200_unet_get_grads(const fmvd_b200_unet *net, float *h_grads);
 int fmvd_b200_unet_forward(fmvd_b200_unet *net, const void *d_views, size_t view_stride, int nplanes,
                            float *d_estimate, void *stream);
 /* One step on a batch of at most max_batch planes; *h_loss receives the
- * mean L1 loss (in units of the per-plane scale).  Synchronous. */
+ * mean L1 loss (in units of the per-plane scale).  Adam with adaptive
+ * gradient clipping: a gradient whose L2 norm exceeds twice the running mean
+ * of earlier steps' norms is scaled down to it, and a step with a non-finite
+ * norm changes nothing.  lr = 0 computes the gradients only.  Synchronous. */
 int fmvd_b200_unet_train_step(fmvd_b200_unet *net, const void *d_views, size_t view_stride, int nplanes,
                               const float *d_target, float lr, float *h_loss, void *stream);
 /* Synchronises and reports whether a tensor-core wait timed out. */
