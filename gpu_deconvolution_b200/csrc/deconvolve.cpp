@@ -11,15 +11,62 @@
 // batches compute, the host hands the oldest finished batch to the datasink
 // and pulls the next one from the datasource into its slot, so host I/O
 // overlaps the device work; uploads and downloads run on their own streams.
+// The pinned batch buffers outlive their plan in a process-wide pool, so a
+// caller that creates one plan per volume (as the plugin does) pins host
+// memory once.
 #include "fmvd_internal.h"
 
 #include <stdlib.h>
 #include <string.h>
+#include <mutex>
+#include <utility>
 #include <vector>
 
 namespace fmvd {
 
 namespace {
+
+// Pinned host buffers released by streaming plans, for later plans of the
+// process: pinning (and unpinning) tens of MB takes tens of ms, longer than
+// a small volume's whole deconvolution.  At most kPoolBytes stay cached.
+constexpr size_t kPoolBytes = size_t(1) << 30;
+std::mutex g_pool_lock;
+std::vector<std::pair<size_t, void *>> g_pool;  // (bytes, buffer)
+size_t g_pool_total = 0;
+
+void *pinned_acquire(size_t bytes)
+{
+    {
+        std::lock_guard<std::mutex> lk(g_pool_lock);
+        int best = -1;
+        for (int i = 0; i < (int)g_pool.size(); i++)
+            if (g_pool[i].first >= bytes && (best < 0 || g_pool[i].first < g_pool[best].first))
+                best = i;
+        if (best >= 0) {
+            void *p = g_pool[best].second;
+            g_pool_total -= g_pool[best].first;
+            g_pool.erase(g_pool.begin() + best);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    return FMVD_CHECK(cudaMallocHost(&p, bytes)) ? p : nullptr;
+}
+
+void pinned_release(void *p, size_t bytes)
+{
+    if (!p)
+        return;
+    {
+        std::lock_guard<std::mutex> lk(g_pool_lock);
+        if (g_pool_total + bytes <= kPoolBytes) {
+            g_pool.emplace_back(bytes, p);
+            g_pool_total += bytes;
+            return;
+        }
+    }
+    cudaFreeHost(p);
+}
 
 template <typename S>
 struct Traits;
@@ -60,6 +107,7 @@ struct Streamer {
     size_t plane = 0;
     struct Slot {
         S *h_in = nullptr, *d_in = nullptr, *h_out = nullptr, *d_out = nullptr;
+        size_t in_bytes = 0, out_bytes = 0;
         std::vector<S *> view_ptrs;
         int n = 0;       // planes of the batch held (0: free)
         cudaEvent_t up = nullptr, done = nullptr, down = nullptr;
@@ -95,13 +143,16 @@ struct Streamer {
             Slot &sl = slot[k];
             const size_t in_bytes = sizeof(S) * plane * cap_planes * V;
             const size_t out_bytes = sizeof(S) * plane * cap_planes;
-            ok = FMVD_CHECK(cudaMallocHost(&sl.h_in, in_bytes)) && FMVD_CHECK(cudaMalloc(&sl.d_in, in_bytes)) &&
-                 FMVD_CHECK(cudaMallocHost(&sl.h_out, out_bytes)) && FMVD_CHECK(cudaMalloc(&sl.d_out, out_bytes)) &&
+            sl.h_in = (S *)pinned_acquire(in_bytes);
+            sl.in_bytes = sl.h_in ? in_bytes : 0;
+            sl.h_out = sl.h_in ? (S *)pinned_acquire(out_bytes) : nullptr;
+            sl.out_bytes = sl.h_out ? out_bytes : 0;
+            ok = sl.h_in && sl.h_out && FMVD_CHECK(cudaMalloc(&sl.d_in, in_bytes)) &&
+                 FMVD_CHECK(cudaMalloc(&sl.d_out, out_bytes)) &&
                  FMVD_CHECK(cudaEventCreateWithFlags(&sl.up, cudaEventDisableTiming)) &&
                  FMVD_CHECK(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming)) &&
                  FMVD_CHECK(cudaEventCreateWithFlags(&sl.down, cudaEventDisableTiming));
-            if (ok) {
-                memset(sl.h_in, 0, in_bytes);
+            if (ok) {  // no clearing: only planes the datasource wrote are uploaded
                 sl.view_ptrs.resize(V);
                 for (int v = 0; v < V; v++)
                     sl.view_ptrs[v] = sl.h_in + (size_t)v * cap_planes * plane;
@@ -113,9 +164,9 @@ struct Streamer {
     void release()
     {
         for (auto &sl : slot) {
-            cudaFreeHost(sl.h_in);
+            pinned_release(sl.h_in, sl.in_bytes);
             cudaFree(sl.d_in);
-            cudaFreeHost(sl.h_out);
+            pinned_release(sl.h_out, sl.out_bytes);
             cudaFree(sl.d_out);
             if (sl.up) cudaEventDestroy(sl.up);
             if (sl.done) cudaEventDestroy(sl.done);
