@@ -174,6 +174,24 @@ def test_streaming_c_callbacks_match_device_api():
     assert stats["source_calls"] == 14 and stats["sink_calls"] == 13
 
 
+def test_streaming_plans_reuse_pinned_buffers():
+    """Streaming plans hand their pinned batch buffers to a process-wide pool
+    that later plans draw from without clearing them: a plan that follows
+    plans over other data, including a source shorter than nstreams (whose
+    missing planes the reference leaves as zeros), gives the same planes as
+    the same plan run first."""
+    a_views, psfs, weights, _ = synth.plain_rl_views(shape=(11, 40, 44), n_views=3, n_beads=10, ksize=9, seed=18)
+    b_views, _, _, _ = synth.plain_rl_views(shape=(2, 40, 44), n_views=3, n_beads=10, ksize=9, seed=19)
+    first_b = api.deconvolve_c_callbacks(b_views, weights, [p.copy() for p in psfs], 0, 3, nstreams=3)
+    first_a = api.deconvolve_c_callbacks(a_views, weights, [p.copy() for p in psfs], 0, 3, nstreams=3)
+    for _ in range(2):
+        assert np.array_equal(api.deconvolve_c_callbacks(b_views, weights, [p.copy() for p in psfs], 0, 3,
+                                                         nstreams=3), first_b)
+        assert np.array_equal(api.deconvolve_c_callbacks(a_views, weights, [p.copy() for p in psfs], 0, 3,
+                                                         nstreams=3), first_a)
+    assert first_b.shape[0] == 3  # the quirk plane of a 2-plane source with nstreams 3
+
+
 def test_streaming_strict_read_ahead(monkeypatch):
     """FMVD_STRICT_READ_AHEAD=1: the datasource never runs more than nstreams
     planes ahead of the datasink (the reference's read-ahead), and the planes
