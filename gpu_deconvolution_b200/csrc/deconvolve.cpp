@@ -28,7 +28,8 @@ namespace {
 
 // Pinned host buffers released by streaming plans, for later plans of the
 // process: pinning (and unpinning) tens of MB takes tens of ms, longer than
-// a small volume's whole deconvolution.  At most kPoolBytes stay cached.
+// a small volume's whole deconvolution.  At most kPoolBytes stay cached;
+// buffers that a device reset released are dropped when found.
 constexpr size_t kPoolBytes = size_t(1) << 30;
 std::mutex g_pool_lock;
 std::vector<std::pair<size_t, void *>> g_pool;  // (bytes, buffer)
@@ -39,9 +40,15 @@ void *pinned_acquire(size_t bytes)
     {
         std::lock_guard<std::mutex> lk(g_pool_lock);
         int best = -1;
-        for (int i = 0; i < (int)g_pool.size(); i++)
+        for (int i = 0; i < (int)g_pool.size(); i++) {
+            if (!pinned_still_valid(g_pool[i].second)) {  // released by a device reset: forget it
+                g_pool_total -= g_pool[i].first;
+                g_pool.erase(g_pool.begin() + i--);
+                continue;
+            }
             if (g_pool[i].first >= bytes && (best < 0 || g_pool[i].first < g_pool[best].first))
                 best = i;
+        }
         if (best >= 0) {
             void *p = g_pool[best].second;
             g_pool_total -= g_pool[best].first;
@@ -381,6 +388,16 @@ void *pinned_malloc(size_t size)
 }
 
 void pinned_free(void *p) { cudaFreeHost(p); }
+
+bool pinned_still_valid(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
 
 fmvd_plan_cuda_16 *initialize_16(int dataH, int dataW, const float *const *w, float **k, int kH, int kW, int type,
                                  int V, int nstreams, datasource_16_t src, datasink_16_t sink, int pairs_cap)

@@ -86,6 +86,10 @@ void engine_batch(Engine *e, const void *data, size_t view_stride, void *out, in
 // ---- plans and streaming (deconvolve.cpp)
 void *pinned_malloc(size_t size);
 void pinned_free(void *p);
+// Whether p is still a pinned host allocation of the process's CUDA context.
+// Pinned buffers kept for reuse are checked with it: cudaDeviceReset releases
+// them behind the cache's back.
+bool pinned_still_valid(const void *p);
 fmvd_plan_cuda_16 *initialize_16(int dataH, int dataW, const float *const *w, float **k, int kH, int kW, int type,
                                  int V, int nstreams, datasource_16_t src, datasink_16_t sink, int pairs_cap);
 fmvd_plan_cuda_8 *initialize_8(int dataH, int dataW, const float *const *w, float **k, int kH, int kW, int type,

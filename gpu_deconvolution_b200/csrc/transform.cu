@@ -513,6 +513,10 @@ std::unique_lock<std::mutex> staging_lock() { return std::unique_lock<std::mutex
 
 void *staging_buffer(int i, size_t bytes)
 {
+    if (g_stage[i] && !pinned_still_valid(g_stage[i])) {  // released by a device reset
+        g_stage[i] = nullptr;
+        g_stage_bytes[i] = 0;
+    }
     if (g_stage_bytes[i] < bytes) {
         cudaFreeHost(g_stage[i]);
         g_stage[i] = nullptr;
