@@ -173,8 +173,11 @@ int fmvd_b200_reconstruct_host(fmvd_b200_reconstructor *r, const void *const *h_
             fmvd::host_copy((char *)h_out + (size_t)k * r->chunk * plane, r->stage[b], planes_of(k) * plane);
     }
     int status = 0;
-    ok = ok && FMVD_CHECK(cudaStreamSynchronize(r->rs)) && FMVD_CHECK(cudaStreamSynchronize(r->comp)) &&
-         FMVD_CHECK(cudaMemcpy(&status, r->status, sizeof(int), cudaMemcpyDeviceToHost));
+    // everything queued has finished before returning, also after a failure:
+    // the copies read the caller's views
+    const bool idle = FMVD_CHECK(cudaStreamSynchronize(r->rs)) & FMVD_CHECK(cudaStreamSynchronize(r->comp)) &
+                      FMVD_CHECK(cudaStreamSynchronize(r->copy));
+    ok = ok && idle && FMVD_CHECK(cudaMemcpy(&status, r->status, sizeof(int), cudaMemcpyDeviceToHost));
     if (ok && status) {
         fmvd::report_error("fmvd: a resampler brick load did not complete in time");
         ok = false;
