@@ -54,7 +54,7 @@ def lib():
 
 @pytest.fixture(scope="session")
 def ref_lib():
-    """The reference library built from the upstream sources (GPU box only)."""
+    """The reference library built from the upstream sources (runs on a GPU)."""
     from oracle import ref_lib as R
     if not R.available():
         pytest.skip("reference build not present")
