@@ -4,17 +4,18 @@
 // which binds the source to a 3-D texture and fetches every target voxel with
 // hardware trilinear filtering.  Here the source lives in plain device memory
 // (rows padded to 16 bytes) described by a 3-D TMA tensor map.  Each CTA
-// resamples a 32 x 8 tile of a stack of up to 8 consecutive target planes:
+// resamples a 32 x 8 tile of a stack of up to 16 consecutive target planes:
 // since the map is affine, every stack's source footprint has the same shape,
 // so the host sizes one box that covers it (with slack for rounding), one
 // thread issues a single cp.async.bulk.tensor load of that brick into shared
 // memory (out-of-volume texels arrive as zeros, the texture's border colour),
 // and the threads interpolate every plane of the stack from shared memory.
 // Consecutive target planes sample overlapping source footprints, so one
-// brick per stack moves a fraction of the bytes of one brick per plane.  The interpolation follows the texture
-// unit's linear filter: texel centres at i + 0.5, weights held with 8
-// fractional bits, values normalised by 2^bits - 1; output quantised as the
-// reference does, (sample)(v * 2^bits + 0.5) through a 32-bit integer.
+// brick per stack moves a fraction of the bytes of one brick per plane.  The
+// interpolation follows the texture unit's linear filter: texel centres at
+// i + 0.5, weights held with 8 fractional bits, values normalised by
+// 2^bits - 1; output quantised as the reference does,
+// (sample)(v * 2^bits + 0.5) through a 32-bit integer.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
