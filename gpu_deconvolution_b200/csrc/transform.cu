@@ -330,7 +330,7 @@ bool resample_device(int bits, const void *d_src, size_t pitch, int w, int h, in
     // box covering the footprint of a stack of kz tiles: extent + 2 texels
     // for the filter and slack, one more so that every texel of the stack is
     // in the brick with one to spare, plus the alignment of the x origin; kz
-    // is the deepest stack (8, 4, 2 or 1 target planes) whose box fits
+    // is the deepest stack (16, 8, 4, 2 or 1 target planes) whose box fits
     int box[3] = {0, 0, 0};
     int kz = kMaxStack;
     size_t smem = 0;
